@@ -1,0 +1,155 @@
+/* C ABI of libfvm_b200: the B200 finite-volume residual + Runge-Kutta stage path.
+ *
+ * The reference (nathanzimniak/multiphysics-fvm) is pure Python/NumPy and has no
+ * FFI; these entry points are what its Python surface binds to (by ctypes) when a
+ * setup selects this backend.  Each declaration names the reference interface it
+ * replaces.  All calls return 0 on success or a negative FVM_E_* code; the message
+ * of the last failure on the calling thread is available from fvm_last_error().
+ * No C++ exception crosses this boundary.  A handle owns all of its device memory
+ * and one CUDA stream; it is not thread-safe, separate handles are independent.
+ *
+ * Host arrays are float64, C-contiguous, in the reference's own layout: one
+ * variable is an (nx1+2, nx2+2, nx3+2) array with one ghost layer
+ * (src/physics/navier_stokes.py:33-39); a whole state is (NV, nx1+2, nx2+2, nx3+2)
+ * with variables in the reference's allocate_u order.
+ */
+#ifndef FVM_B200_H
+#define FVM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FVM_OK 0
+#define FVM_E_INVALID (-1)   /* bad argument or unsupported combination (ValueError) */
+#define FVM_E_CUDA (-2)      /* CUDA runtime/driver failure */
+#define FVM_E_NOMEM (-3)     /* device or pinned allocation failed */
+#define FVM_E_STATE (-4)     /* status word non-zero (NaN, rho<=0, P<=0, dt<=0, timeout) */
+
+/* physics (setup["physics"] module) */
+#define FVM_NAVIER_STOKES 0
+#define FVM_HEAT 1
+#define FVM_MAXWELL 2
+/* coordinate systems (src/grid/geometry.py:14) */
+#define FVM_CARTESIAN 0
+#define FVM_CYLINDRICAL 1
+#define FVM_SPHERICAL 2
+/* space schemes (src/numerics/*.py) */
+#define FVM_PIECEWISE_CONSTANT 0
+#define FVM_MUSCL 1
+#define FVM_MINMOD 0
+#define FVM_MONOTONIZED_CENTRAL 1
+#define FVM_VAN_LEER 2
+#define FVM_RUSANOV 0
+#define FVM_HLL 1
+/* time integrators (src/numerics/time_integrators.py) */
+#define FVM_EULER_EXPLICIT 0
+#define FVM_RK3 1
+#define FVM_RK3_SSP 2
+#define FVM_RK4 3
+/* boundary conditions (src/grid/boundary_conditions.py) + Dirichlet (new) */
+#define FVM_BC_PERIODIC 0
+#define FVM_BC_NEUMANN 1
+#define FVM_BC_REFLECTING 2
+#define FVM_BC_DIRICHLET 3
+/* precision of the device state and stencil arithmetic */
+#define FVM_FP32 0
+#define FVM_FP64 1
+/* status bits (fvm_status) */
+#define FVM_ST_NONFINITE 1u
+#define FVM_ST_DENSITY 2u
+#define FVM_ST_PRESSURE 4u
+#define FVM_ST_DT 8u
+#define FVM_ST_TIMEOUT 16u
+
+/* Everything a setup dict selects (setups/kelvin_helmholtz.py:154-163).
+ * params: navier_stokes {gamma, mu, g1, g2, g3}; heat {rho, cp, k, q};
+ *         maxwell {mu, epsilon, sigma, rho_c, chi_B, chi_D}.
+ * bc_kind/bc_value: [variable][side], sides ordered left,right,bottom,top,front,back
+ * (src/solver.py:36).  tile_ty / zchunk: 0 = autotuned default. */
+typedef struct fvm_desc {
+  int physics, precision, coords;
+  int nx1, nx2, nx3;
+  double x1_min, x1_max, x2_min, x2_max, x3_min, x3_max;
+  int reconstructor, limiter, riemann, integrator;
+  int bc_kind[6][6];
+  double bc_value[6][6];
+  double params[8];
+  int tile_ty, zchunk;
+} fvm_desc;
+
+typedef struct fvm_handle fvm_handle;
+
+/* Build the grid + device state for a setup.
+ * Replaces geometry.build_grid (src/grid/geometry.py:14-194) and
+ * physics.allocate_u (src/physics/navier_stokes.py:13-41) as called by
+ * src/solver.py:125-128. */
+int fvm_create(const fvm_desc* desc, fvm_handle** out);
+
+/* Release every device/pinned buffer, graph and stream of the handle. */
+int fvm_destroy(fvm_handle* h);
+
+/* Number of conserved variables and the device buffer footprint in bytes. */
+int fvm_info(const fvm_handle* h, int* nvars, long long* device_bytes);
+
+/* Copy a whole ghosted host state (NV, nx1+2, nx2+2, nx3+2) to the device.
+ * Replaces the host-resident U dict written by apply_ics (src/solver.py:64-85). */
+int fvm_upload(fvm_handle* h, const double* host_state);
+
+/* Copy the device state back into a ghosted host array (NV, nx1+2, nx2+2, nx3+2).
+ * Ghost faces are refreshed from the boundary conditions and ghost edges/corners
+ * averaged as in src/solver.py:39-61.  Replaces reading U in io.save_snapshot
+ * (src/io.py:14-63). */
+int fvm_download(fvm_handle* h, double* host_state);
+
+/* dt = CFL / max characteristic rate of the current state, reduced on the device
+ * in float64.  Replaces physics.compute_dt (navier_stokes.py:512-585,
+ * heat.py:305-351, maxwell.py:533-600). */
+int fvm_compute_dt(fvm_handle* h, double cfl, double* dt_out);
+
+/* Residual of the uploaded state exactly as given (ghosts are not refilled),
+ * written into host_rhs (NV, nx1, nx2, nx3).  Replaces physics.compute_rhs
+ * (navier_stokes.py:588-711, heat.py:354-473, maxwell.py:603-729). */
+int fvm_residual(fvm_handle* h, double* host_rhs);
+
+/* Advance n_steps time steps on the device (each step captured once as a CUDA
+ * graph: [dt reduction] + per stage {ghost fill, fused stage kernel}).
+ * dt_mode 0: dt = compute_dt(cfl) every step, stopping (as no-op steps) once
+ * t > t_end (src/solver.py:137-150).  dt_mode 1: the fixed dt of fvm_set_dt.
+ * Replaces the time loop body src/solver.py:140-143 and the integrators
+ * euler_explicit/rk3/rk3_ssp/rk4 (src/numerics/time_integrators.py:10-221)
+ * together with apply_bcs (src/solver.py:13-61). */
+int fvm_step(fvm_handle* h, int n_steps, int dt_mode);
+
+/* Same as fvm_step without the final synchronisation of the host, returning the
+ * device time of the n_steps graph launches (CUDA events on the handle's stream). */
+int fvm_time_steps(fvm_handle* h, int n_steps, int dt_mode, double* ms);
+
+/* Configure the time loop: CFL number, end time (inf = step-counted) and fixed dt. */
+int fvm_set_time(fvm_handle* h, double t, double t_end, double cfl);
+int fvm_set_dt(fvm_handle* h, double dt);
+
+/* Simulated time, steps taken and the last dt (read back from the device). */
+int fvm_get_time(fvm_handle* h, double* t, long long* steps, double* last_dt);
+
+/* Conserved totals sum(U*V) over the interior in float64 with compensated
+ * summation (NV values; Maxwell adds the EM energy 0.5(D.E+B.H)V as entry NV).
+ * New: the reference has no such diagnostic. */
+int fvm_totals(fvm_handle* h, double* totals);
+
+/* Sticky device status word (FVM_ST_* bits); fvm_clear_status resets it. */
+int fvm_status(fvm_handle* h, unsigned* status);
+int fvm_clear_status(fvm_handle* h);
+
+/* Per-launch device time of the stage kernels (ms, CUDA events on the handle's
+ * stream) over n_steps un-captured steps; fills per-stage totals. */
+int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_kernel_ms,
+                      double* other_kernel_ms, int* stage_launches);
+
+/* Copy the message of the last failure on this thread into buf. */
+int fvm_last_error(char* buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FVM_B200_H */

@@ -1,0 +1,290 @@
+"""Setup dict -> device simulation handle.
+
+A setup (the reference's plugin surface, e.g. setups/kelvin_helmholtz.py:154-163)
+selects its physics module, integrator, space schemes and boundary conditions
+as Python callables.  This module maps those callables - this package's own or
+the reference's functions of the same name - onto the enums of ``fvm_desc`` and
+owns the device handle.  Unknown choices raise ``ValueError`` before anything
+is launched, as the reference does (geometry.py:173, boundary_conditions.py:37).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from collections import OrderedDict
+
+import numpy as np
+
+from . import _lib as L
+
+VARIABLES = {
+    "navier_stokes": ("mass_density", "momentum_x1", "momentum_x2", "momentum_x3", "energy_density"),
+    "heat": ("internal_energy_density",),
+    "maxwell": ("magnetic_field_x1", "magnetic_field_x2", "magnetic_field_x3",
+                "electric_d_field_x1", "electric_d_field_x2", "electric_d_field_x3"),
+}
+PHYSICS_ID = {"navier_stokes": L.NAVIER_STOKES, "heat": L.HEAT, "maxwell": L.MAXWELL}
+COORDS = {"cartesian": L.CARTESIAN, "cylindrical": L.CYLINDRICAL, "spherical": L.SPHERICAL}
+SIDES = ("left", "right", "bottom", "top", "front", "back")
+
+# kind -> (module basename, {function name: enum})
+SCHEMES = {
+    "riemann_solver": ("riemann_solvers", {"rusanov": L.RUSANOV, "hll": L.HLL}),
+    "reconstructor": ("reconstructors", {"piecewise_constant": L.PIECEWISE_CONSTANT, "muscl": L.MUSCL}),
+    "slope_limiter": ("slope_limiters", {"minmod": L.MINMOD, "monotonized_central": L.MONOTONIZED_CENTRAL,
+                                         "van_leer": L.VAN_LEER}),
+    "diffusive_solver": ("diffusive_solvers", {"centered": 0}),
+    "time_integrator": ("time_integrators", {"euler_explicit": L.EULER_EXPLICIT, "rk3": L.RK3,
+                                             "rk3_ssp": L.RK3_SSP, "rk4": L.RK4}),
+    "boundary_condition": ("boundary_conditions", {"periodic": L.BC_PERIODIC, "neumann": L.BC_NEUMANN,
+                                                   "reflecting": L.BC_REFLECTING}),
+}
+
+
+def scheme_id(kind: str, fn):
+    """Enum of a scheme callable: this package's callables carry ``_fvm_id``;
+    the reference's are recognised by module and function name."""
+    fid = getattr(fn, "_fvm_id", None)
+    if fid is not None and fid[0] == kind:
+        return fid[1]
+    mod, table = SCHEMES[kind]
+    name = getattr(fn, "__name__", None)
+    modname = (getattr(fn, "__module__", "") or "").split(".")[-1]
+    if name in table and modname == mod:
+        return table[name]
+    raise ValueError(f"Unknown {kind.replace('_', ' ')}: {fn!r}")
+
+
+def physics_name(module) -> str:
+    """'navier_stokes' | 'heat' | 'maxwell' for a physics module (ours or the reference's)."""
+    name = getattr(module, "PHYSICS", None) or (getattr(module, "__name__", "") or "").split(".")[-1]
+    if name not in PHYSICS_ID:
+        raise ValueError(f"Unknown physics module: {module!r}")
+    return name
+
+
+def physics_params(name: str, p: dict) -> list[float]:
+    """Ordered parameters of fvm_desc.params (include/fvm.h)."""
+    if name == "navier_stokes":
+        g = p["gravitational_acceleration"]
+        return [p["heat_capacity_ratio"], p["dynamic_viscosity"], g[0], g[1], g[2]]
+    if name == "heat":
+        return [p["mass_density"], p["specific_heat_capacity"], p["thermal_conductivity"],
+                p["volumetric_heat_source"]]
+    return [p["magnetic_permeability"], p["electric_permittivity"], p["electrical_conductivity"],
+            p["charge_density"], p["magnetic_cleaning_coeff"], p["electric_cleaning_coeff"]]
+
+
+def bc_codes(name: str, bcs: dict):
+    """[var][side] -> (kind, value) for every variable of the physics."""
+    out = []
+    for var in VARIABLES[name]:
+        per = bcs[var]
+        row = []
+        for side in SIDES:
+            fid = scheme_id("boundary_condition", per[side])
+            row.append(fid if isinstance(fid, tuple) else (fid, 0.0))
+        out.append(row)
+    return out
+
+
+def _key(x):
+    if isinstance(x, dict):
+        return tuple(sorted((k, _key(v)) for k, v in x.items()))
+    if isinstance(x, (list, tuple)):
+        return tuple(_key(v) for v in x)
+    if callable(x):
+        return (getattr(x, "__module__", None), getattr(x, "__name__", None), getattr(x, "_fvm_id", None))
+    return x
+
+
+class Simulation:
+    """One device-resident simulation (an ``fvm_handle``).
+
+    State arrays cross the boundary in the reference's layout: float64,
+    ``(NV, nx1+2, nx2+2, nx3+2)`` with one ghost layer.
+    """
+
+    def __init__(self, physics: str, coordinate_system: str, grid_config: dict, params: dict,
+                 space_schemes: dict, bcs: dict, integrator=None, precision: str = "fp64",
+                 zchunk: int = 0, tile_ty: int = 0):
+        lib = L.load()
+        self.physics = physics
+        self.nv = len(VARIABLES[physics])
+        self.variables = VARIABLES[physics]
+        self.n = (int(grid_config["nx1"]), int(grid_config["nx2"]), int(grid_config["nx3"]))
+        if coordinate_system not in COORDS:
+            raise ValueError(f"Unknown coordinate system: '{coordinate_system}'. "
+                             "Expected one of: cartesian, cylindrical, spherical.")
+        if precision not in ("fp32", "fp64"):
+            raise ValueError(f"Unknown precision {precision!r} (fp32 or fp64)")
+        d = L.FvmDesc()
+        d.physics = PHYSICS_ID[physics]
+        d.precision = L.FP64 if precision == "fp64" else L.FP32
+        d.coords = COORDS[coordinate_system]
+        d.nx1, d.nx2, d.nx3 = self.n
+        for ax in (1, 2, 3):
+            setattr(d, f"x{ax}_min", float(grid_config[f"x{ax}_min"]))
+            setattr(d, f"x{ax}_max", float(grid_config[f"x{ax}_max"]))
+        d.reconstructor = scheme_id("reconstructor", space_schemes["reconstructor"])
+        lim = space_schemes.get("slope_limiter")
+        d.limiter = scheme_id("slope_limiter", lim) if lim is not None else L.MINMOD
+        if physics != "heat":
+            d.riemann = scheme_id("riemann_solver", space_schemes["riemann_solver"])
+        if physics != "maxwell" and "diffusive_solver" in space_schemes:
+            scheme_id("diffusive_solver", space_schemes["diffusive_solver"])
+        d.integrator = scheme_id("time_integrator", integrator) if integrator is not None else L.RK3_SSP
+        for q, row in enumerate(bc_codes(physics, bcs)):
+            for s, (kind, value) in enumerate(row):
+                d.bc_kind[q][s] = kind
+                d.bc_value[q][s] = float(value)
+        for i, v in enumerate(physics_params(physics, params)):
+            d.params[i] = float(v)
+        d.zchunk = int(zchunk)
+        d.tile_ty = int(tile_ty)
+        self.desc = d
+        self.precision = precision
+        h = C.c_void_p()
+        L.check(lib.fvm_create(C.byref(d), C.byref(h)), "fvm_create")
+        self._h = h
+        self._lib = lib
+        self._ghosted = (self.nv,) + tuple(x + 2 for x in self.n)
+
+    # -- life cycle --------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.fvm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @classmethod
+    def from_setup(cls, setup: dict, **kw):
+        name = physics_name(setup["physics"])
+        return cls(name, setup["coordinate_system"], setup["grid_config"], setup["physical_parameters"],
+                   setup["space_schemes"], setup["boundary_conditions"], setup.get("time_integrator"),
+                   precision=setup.get("precision", "fp64"), **kw)
+
+    # -- state transfer ----------------------------------------------------
+    def _stack(self, U) -> np.ndarray:
+        if isinstance(U, dict):
+            arr = np.stack([np.asarray(U[k], dtype=np.float64) for k in self.variables])
+        else:
+            arr = np.asarray(U, dtype=np.float64)
+        if arr.shape != self._ghosted:
+            raise ValueError(f"state shape {arr.shape} != {self._ghosted}")
+        return np.ascontiguousarray(arr)
+
+    def upload(self, U):
+        arr = self._stack(U)
+        L.check(self._lib.fvm_upload(self._h, L.dptr(arr)), "fvm_upload")
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self._ghosted, dtype=np.float64)
+        L.check(self._lib.fvm_download(self._h, L.dptr(out)), "fvm_download")
+        return out
+
+    def download_into(self, U: dict):
+        arr = self.download()
+        for q, k in enumerate(self.variables):
+            U[k][...] = arr[q]
+
+    # -- hot path ------------------------------------------------------------
+    def residual(self) -> np.ndarray:
+        out = np.empty((self.nv,) + self.n, dtype=np.float64)
+        L.check(self._lib.fvm_residual(self._h, L.dptr(out)), "fvm_residual")
+        return out
+
+    def compute_dt(self, cfl: float) -> float:
+        dt = C.c_double()
+        L.check(self._lib.fvm_compute_dt(self._h, float(cfl), C.byref(dt)), "fvm_compute_dt")
+        return dt.value
+
+    def set_time(self, t: float = 0.0, t_end: float = math.inf, cfl: float = 0.4):
+        L.check(self._lib.fvm_set_time(self._h, float(t), float(t_end), float(cfl)), "fvm_set_time")
+
+    def step(self, n_steps: int = 1, dt: float | None = None):
+        """Advance n_steps; dt=None uses the device CFL step (fvm_set_time's cfl)."""
+        if dt is not None:
+            L.check(self._lib.fvm_set_dt(self._h, float(dt)), "fvm_set_dt")
+        L.check(self._lib.fvm_step(self._h, int(n_steps), 0 if dt is None else 1), "fvm_step")
+
+    def time_steps(self, n_steps: int, fixed_dt: bool = False) -> float:
+        ms = C.c_double()
+        L.check(self._lib.fvm_time_steps(self._h, int(n_steps), 1 if fixed_dt else 0, C.byref(ms)),
+                "fvm_time_steps")
+        return ms.value
+
+    def profile_steps(self, n_steps: int, fixed_dt: bool = False):
+        st, ot, nl = C.c_double(), C.c_double(), C.c_int()
+        L.check(self._lib.fvm_profile_steps(self._h, int(n_steps), 1 if fixed_dt else 0, C.byref(st),
+                                            C.byref(ot), C.byref(nl)), "fvm_profile_steps")
+        return st.value, ot.value, nl.value
+
+    def time(self):
+        t, dt, n = C.c_double(), C.c_double(), C.c_longlong()
+        L.check(self._lib.fvm_get_time(self._h, C.byref(t), C.byref(n), C.byref(dt)), "fvm_get_time")
+        return t.value, n.value, dt.value
+
+    def totals(self) -> np.ndarray:
+        nt = self.nv + (1 if self.physics == "maxwell" else 0)
+        out = np.zeros(8, dtype=np.float64)
+        L.check(self._lib.fvm_totals(self._h, L.dptr(out)), "fvm_totals")
+        return out[:nt]
+
+    def status(self) -> int:
+        s = C.c_uint()
+        L.check(self._lib.fvm_status(self._h, C.byref(s)), "fvm_status")
+        return s.value
+
+    def clear_status(self):
+        L.check(self._lib.fvm_clear_status(self._h), "fvm_clear_status")
+
+    def info(self):
+        nv, nb = C.c_int(), C.c_longlong()
+        L.check(self._lib.fvm_info(self._h, C.byref(nv), C.byref(nb)), "fvm_info")
+        return nv.value, nb.value
+
+
+class _Cache:
+    """Small LRU of simulations for the functional drop-in API (compute_rhs,
+    compute_dt, integrators), keyed by everything that shapes the handle."""
+
+    def __init__(self, size=4):
+        self.size = size
+        self.d: OrderedDict = OrderedDict()
+
+    def get(self, key, make):
+        if key in self.d:
+            self.d.move_to_end(key)
+            return self.d[key]
+        sim = make()
+        self.d[key] = sim
+        while len(self.d) > self.size:
+            _, old = self.d.popitem(last=False)
+            old.close()
+        return sim
+
+
+CACHE = _Cache()
+
+
+def cached_simulation(physics: str, grid: dict, params: dict, space_schemes: dict, bcs=None,
+                      integrator=None, precision: str | None = None) -> Simulation:
+    cs = grid.get("coordinate_system")
+    if cs is None:
+        raise ValueError("grid dict lacks 'coordinate_system': build it with multiphysics_fvm_b200.grid.geometry.build_grid")
+    prec = precision or grid.get("precision", "fp64")
+    if bcs is None:  # residual-only use: any valid BC set
+        p = ("periodic",)
+        from .grid import boundary_conditions as bcm
+        bcs = {v: {s: bcm.periodic for s in SIDES} for v in VARIABLES[physics]}
+        del p
+    key = (physics, cs, _key(grid["config"]), _key(params), _key(space_schemes), _key(bcs), _key(integrator), prec)
+    return CACHE.get(key, lambda: Simulation(physics, cs, grid["config"], params, space_schemes, bcs,
+                                             integrator, precision=prec))

@@ -1,0 +1,779 @@
+// C ABI of libfvm_b200 (declared in include/fvm.h): handle life cycle, layout
+// transforms, the device-resident time loop (CUDA graphs), CFL reduction and
+// conserved totals.  The stencil work is in the fused stage kernels.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/fvm.h"
+#include "fvm_aux.cuh"
+#include "launch.cuh"
+
+using namespace fvm;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define FVM_CK(x)                                                                                \
+  do {                                                                                           \
+    cudaError_t e_ = (x);                                                                        \
+    if (e_ != cudaSuccess) return fail(FVM_E_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Host copy of the per-axis metric tables (float64), built with the
+// reference's expressions (src/grid/geometry.py:37-171).
+struct HostMetric {
+  std::vector<double> dx1, dx2, dx3, r_c, r_f, r_f2, a1, b1, inv_r, two_inv_r, c2, sin_f2, sin_c2, cot_c2;
+  std::vector<double> inv_dx1, inv_dx2, inv_dx3, inv_sin_c2;
+};
+
+HostMetric build_metric(const fvm_desc& d) {
+  HostMetric m;
+  const int n[3] = {d.nx1, d.nx2, d.nx3};
+  const double lo[3] = {d.x1_min, d.x2_min, d.x3_min}, hi[3] = {d.x1_max, d.x2_max, d.x3_max};
+  std::vector<double> xc[3], xf[3], dl[3];
+  for (int a = 0; a < 3; ++a) {
+    const double dd = (hi[a] - lo[a]) / n[a];
+    for (int i = 0; i < n[a]; ++i) xc[a].push_back(lo[a] + ((double)i + 0.5) * dd);
+    for (int i = 0; i <= n[a]; ++i) xf[a].push_back(lo[a] + (double)i * dd);
+    for (int i = 0; i < n[a]; ++i) dl[a].push_back(xf[a][i + 1] - xf[a][i]);
+  }
+  m.dx1 = dl[0]; m.dx2 = dl[1]; m.dx3 = dl[2];
+  m.r_c = xc[0]; m.r_f = xf[0];
+  for (int i = 0; i <= n[0]; ++i) m.r_f2.push_back(xf[0][i] * xf[0][i]);
+  for (int i = 0; i < n[0]; ++i) {
+    const double p = xf[0][i + 1], q = xf[0][i];
+    m.a1.push_back((p * p - q * q) / 2.0);
+    m.b1.push_back((std::pow(p, 3.0) - std::pow(q, 3.0)) / 3.0);
+    m.inv_r.push_back(1.0 / xc[0][i]);
+    m.two_inv_r.push_back(2.0 / xc[0][i]);
+  }
+  for (int j = 0; j < n[1]; ++j) {
+    m.c2.push_back(std::cos(xf[1][j]) - std::cos(xf[1][j + 1]));
+    m.sin_c2.push_back(std::sin(xc[1][j]));
+    m.cot_c2.push_back(1.0 / std::tan(xc[1][j]));
+  }
+  for (int j = 0; j <= n[1]; ++j) m.sin_f2.push_back(std::sin(xf[1][j]));
+  for (double v : m.dx1) m.inv_dx1.push_back(1.0 / v);
+  for (double v : m.dx2) m.inv_dx2.push_back(1.0 / v);
+  for (double v : m.dx3) m.inv_dx3.push_back(1.0 / v);
+  for (double v : m.sin_c2) m.inv_sin_c2.push_back(1.0 / v);
+  return m;
+}
+
+// Cell lengths on the host, same products as Geo<> (geometry.py:80-171).
+void host_lengths(const HostMetric& m, int coords, int i, int j, int k, double L[3]) {
+  L[0] = m.dx1[i];
+  L[1] = coords == FVM_CARTESIAN ? m.dx2[j] : m.r_c[i] * m.dx2[j];
+  L[2] = coords == FVM_SPHERICAL ? (m.r_c[i] * m.sin_c2[j]) * m.dx3[k] : m.dx3[k];
+}
+
+}  // namespace
+
+struct fvm_handle {
+  fvm_desc d{};
+  int nv = 0;
+  bool f64 = false;
+  size_t esz = 4;
+  Layout lay{};
+  int nsm = 148;
+  cudaStream_t stream = nullptr;
+  void* U[3] = {nullptr, nullptr, nullptr};  // base, stage a, stage b
+  void* acc = nullptr;
+  void* met_real = nullptr;     // metric tables in the state precision
+  double* met_f64 = nullptr;    // metric tables in float64 (reductions)
+  Metric<float> mf{};
+  Metric<double> md{};
+  Clock* clk = nullptr;
+  unsigned* status = nullptr;
+  double* partials = nullptr;
+  double* totals_dev = nullptr;
+  double* stage_dev = nullptr;   // reference-layout float64 staging on the device
+  double* stage_host = nullptr;  // pinned staging
+  size_t stage_elems = 0;
+  CUtensorMap tmap[3];
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double max_inv_l2 = 0.0, const_rate = 0.0;
+  int zchunk = 64;
+  long long device_bytes = 0;
+};
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 4D map (x, y, z, var) over one ghosted state buffer.  Box: 40 columns
+// starting 3 cells left of the tile (x coordinate aligned), `rows` rows, one
+// plane, all variables.
+int make_tmap(fvm_handle* h, int b, int rows) {
+  auto enc = get_encode();
+  if (!enc) return fail(FVM_E_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  const Layout& L = h->lay;
+  cuuint64_t dims[4] = {(cuuint64_t)(L.nx + 2 + L.padx), (cuuint64_t)(L.ny + 2), (cuuint64_t)(L.nz + 2),
+                        (cuuint64_t)h->nv};
+  cuuint64_t strides[3] = {(cuuint64_t)(L.pitch * h->esz), (cuuint64_t)(L.plane * h->esz),
+                           (cuuint64_t)(L.var_stride * h->esz)};
+  cuuint32_t box[4] = {40, (cuuint32_t)rows, 1, (cuuint32_t)h->nv};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(&h->tmap[b], h->f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                   h->U[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(FVM_E_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return FVM_OK;
+}
+
+int validate(const fvm_desc* d) {
+  if (!d) return fail(FVM_E_INVALID, "null desc");
+  if (d->physics < FVM_NAVIER_STOKES || d->physics > FVM_MAXWELL)
+    return fail(FVM_E_INVALID, "Unknown physics " + std::to_string(d->physics));
+  if (d->precision != FVM_FP32 && d->precision != FVM_FP64) return fail(FVM_E_INVALID, "unknown precision");
+  if (d->coords < 0 || d->coords > 2)
+    return fail(FVM_E_INVALID, "Unknown coordinate system. Expected one of: cartesian, cylindrical, spherical.");
+  if (d->nx1 < 1 || d->nx2 < 1 || d->nx3 < 1) return fail(FVM_E_INVALID, "grid sizes must be >= 1");
+  if ((long long)d->nx1 * d->nx2 * d->nx3 > (1ll << 31)) return fail(FVM_E_INVALID, "grid too large");
+  if (d->reconstructor < 0 || d->reconstructor > 1) return fail(FVM_E_INVALID, "unknown reconstructor");
+  if (d->limiter < 0 || d->limiter > 2) return fail(FVM_E_INVALID, "unknown slope limiter");
+  if (d->riemann < 0 || d->riemann > 1) return fail(FVM_E_INVALID, "unknown riemann solver");
+  if (d->integrator < 0 || d->integrator > 3) return fail(FVM_E_INVALID, "unknown time integrator");
+  const int nv = d->physics == FVM_NAVIER_STOKES ? 5 : (d->physics == FVM_HEAT ? 1 : 6);
+  for (int q = 0; q < nv; ++q)
+    for (int s = 0; s < 6; ++s) {
+      if (d->bc_kind[q][s] < 0 || d->bc_kind[q][s] > 3) return fail(FVM_E_INVALID, "Unknown boundary condition");
+      const bool p0 = d->bc_kind[q][s & ~1] == FVM_BC_PERIODIC, p1 = d->bc_kind[q][s | 1] == FVM_BC_PERIODIC;
+      if (p0 != p1) return fail(FVM_E_INVALID, "periodic boundaries must be set on both sides of an axis");
+    }
+  return FVM_OK;
+}
+
+int kernel_limiter(const fvm_desc& d) {
+  if (d.reconstructor == FVM_PIECEWISE_CONSTANT) return LIM_PC;
+  return d.limiter == FVM_MINMOD ? LIM_MINMOD : (d.limiter == FVM_MONOTONIZED_CENTRAL ? LIM_MC : LIM_VANLEER);
+}
+
+BcSpec make_bc(const fvm_desc& d, int nv) {
+  BcSpec b{};
+  for (int q = 0; q < 6; ++q)
+    for (int s = 0; s < 6; ++s) {
+      b.kind[q][s] = (signed char)(q < nv ? d.bc_kind[q][s] : 0);
+      b.value[q][s] = d.bc_value[q][s];
+    }
+  return b;
+}
+
+// Stage table of each integrator (time_integrators.py:10-221): input buffer,
+// output buffer, epilogue mode, constants and accumulator update.
+struct StageDef {
+  int in, out, mode, accmode;
+  double ca, cb, w;
+};
+std::vector<StageDef> stage_table(int integrator) {
+  switch (integrator) {
+    case FVM_EULER_EXPLICIT: return {{0, 1, MODE_EULER, ACC_NONE, 0, 0, 0}};
+    case FVM_RK3:
+      return {{0, 1, MODE_AXPY, ACC_SET, 0.5, 0, 0},
+              {1, 2, MODE_AXPY, ACC_ADD, 1.0, 0, 4.0},
+              {2, 0, MODE_FINAL, ACC_NONE, 0, 0, 0}};
+    case FVM_RK3_SSP:
+      return {{0, 1, MODE_AXPY, ACC_NONE, 1.0, 0, 0},
+              {1, 2, MODE_SSP, ACC_NONE, 0.75, 0.25, 0},
+              {2, 0, MODE_SSP, ACC_NONE, 1.0 / 3.0, 2.0 / 3.0, 0}};
+    default:
+      return {{0, 1, MODE_AXPY, ACC_SET, 0.5, 0, 0},
+              {1, 2, MODE_AXPY, ACC_ADD, 0.5, 0, 2.0},
+              {2, 1, MODE_AXPY, ACC_ADD, 1.0, 0, 2.0},
+              {1, 0, MODE_FINAL, ACC_NONE, 0, 0, 0}};
+  }
+}
+
+template <typename Real>
+Metric<Real> metric_ptrs(const Real* base, const fvm_desc& d) {
+  Metric<Real> m;
+  const Real* p = base;
+  auto take = [&](int n) { const Real* r = p; p += n; return r; };
+  m.dx1 = take(d.nx1); m.dx2 = take(d.nx2); m.dx3 = take(d.nx3);
+  m.r_c = take(d.nx1); m.r_f = take(d.nx1 + 1); m.r_f2 = take(d.nx1 + 1);
+  m.a1 = take(d.nx1); m.b1 = take(d.nx1); m.inv_r = take(d.nx1); m.two_inv_r = take(d.nx1);
+  m.c2 = take(d.nx2); m.sin_f2 = take(d.nx2 + 1); m.sin_c2 = take(d.nx2); m.cot_c2 = take(d.nx2);
+  m.inv_dx1 = take(d.nx1); m.inv_dx2 = take(d.nx2); m.inv_dx3 = take(d.nx3); m.inv_sin_c2 = take(d.nx2);
+  return m;
+}
+
+std::vector<double> pack_metric(const HostMetric& m) {
+  std::vector<double> v;
+  for (auto* t : {&m.dx1, &m.dx2, &m.dx3, &m.r_c, &m.r_f, &m.r_f2, &m.a1, &m.b1, &m.inv_r, &m.two_inv_r, &m.c2,
+                  &m.sin_f2, &m.sin_c2, &m.cot_c2, &m.inv_dx1, &m.inv_dx2, &m.inv_dx3, &m.inv_sin_c2})
+    v.insert(v.end(), t->begin(), t->end());
+  return v;
+}
+
+template <typename Real, typename P>
+void fill_common(fvm_handle* h, const StageDef& sd, bool rhs_only, P& p) {
+  p.lay = h->lay;
+  p.met = metric_ptrs<Real>(static_cast<const Real*>(h->met_real), h->d);
+  p.u0 = static_cast<const Real*>(h->U[0]);
+  p.out = static_cast<Real*>(h->U[sd.out]);
+  p.acc = static_cast<Real*>(h->acc);
+  p.dt = &h->clk->dt;
+  p.active = rhs_only ? nullptr : &h->clk->active;
+  p.coef.mode = sd.mode;
+  p.coef.accmode = sd.accmode;
+  p.coef.ca = sd.ca;
+  p.coef.cb = sd.cb;
+  p.coef.wacc = sd.w;
+  p.status = h->status;
+  p.zchunk = h->zchunk;
+}
+
+template <typename Real>
+cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool prepare_only = false) {
+  const fvm_desc& d = h->d;
+  const int nsm = prepare_only ? -1 : h->nsm;
+  if (d.physics == FVM_HEAT) {
+    HeatParams<Real> p{};
+    fill_common<Real>(h, sd, rhs_only, p);
+    p.rho_cp = d.params[0] * d.params[1];
+    p.k = d.params[2];
+    p.q = d.params[3];
+    return launch_heat<Real>(kernel_limiter(d), d.coords, h->tmap[sd.in], p, h->stream, nsm);
+  }
+  if (d.physics == FVM_MAXWELL) {
+    MaxwellParams<Real> p{};
+    fill_common<Real>(h, sd, rhs_only, p);
+    p.mu = d.params[0];
+    p.ep = d.params[1];
+    p.sigma = d.params[2];
+    p.rho_c = d.params[3];
+    p.chi_b = d.params[4];
+    p.chi_d = d.params[5];
+    p.c = 1 / std::sqrt(d.params[0] * d.params[1]);
+    return launch_maxwell<Real>(kernel_limiter(d), d.riemann, d.coords, h->tmap[sd.in], p, h->stream, nsm);
+  }
+  NsParams<Real> p{};
+  p.lay = h->lay;
+  p.met = metric_ptrs<Real>(static_cast<const Real*>(h->met_real), d);
+  p.u0 = static_cast<const Real*>(h->U[0]);
+  p.out = static_cast<Real*>(h->U[sd.out]);
+  p.acc = static_cast<Real*>(h->acc);
+  p.dt = &h->clk->dt;
+  p.active = rhs_only ? nullptr : &h->clk->active;
+  p.coef.mode = sd.mode;
+  p.coef.accmode = sd.accmode;
+  p.coef.ca = sd.ca;
+  p.coef.cb = sd.cb;
+  p.coef.wacc = sd.w;
+  p.gamma = d.params[0];
+  p.mu = d.params[1];
+  p.g1 = d.params[2];
+  p.g2 = d.params[3];
+  p.g3 = d.params[4];
+  p.status = h->status;
+  p.zchunk = h->zchunk;
+  const bool visc = d.params[1] != 0.0;
+  return launch_ns<Real>(kernel_limiter(d), d.riemann, d.coords, visc, h->tmap[sd.in], p, h->stream,
+                         prepare_only ? -1 : h->nsm);
+}
+
+cudaError_t launch_bc(fvm_handle* h, int b, bool use_active) {
+  const Layout& L = h->lay;
+  const long long work = 2ll * h->nv * ((long long)L.ny * L.nz + (long long)L.nx * L.nz + (long long)L.nx * L.ny);
+  int blocks = (int)std::min<long long>((work + 255) / 256, 4096);
+  const BcSpec bc = make_bc(h->d, h->nv);
+  const int* act = use_active ? &h->clk->active : nullptr;
+  if (h->f64) bc_fill_kernel<double><<<blocks, 256, 0, h->stream>>>(static_cast<double*>(h->U[b]), L, h->nv, bc, act);
+  else bc_fill_kernel<float><<<blocks, 256, 0, h->stream>>>(static_cast<float*>(h->U[b]), L, h->nv, bc, act);
+  return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_dt_reduce(fvm_handle* h) {
+  const int blocks = h->nsm * 4;
+  const Real* u = static_cast<const Real*>(h->U[0]);
+  const double g = h->d.params[0], mu = h->d.params[1];
+  switch (h->d.coords) {
+    case FVM_CARTESIAN: ns_dt_reduce_kernel<Real, COORD_CART><<<blocks, 256, 0, h->stream>>>(u, h->lay, h->md, g, mu, h->clk, h->status); break;
+    case FVM_CYLINDRICAL: ns_dt_reduce_kernel<Real, COORD_CYL><<<blocks, 256, 0, h->stream>>>(u, h->lay, h->md, g, mu, h->clk, h->status); break;
+    default: ns_dt_reduce_kernel<Real, COORD_SPH><<<blocks, 256, 0, h->stream>>>(u, h->lay, h->md, g, mu, h->clk, h->status); break;
+  }
+  return cudaGetLastError();
+}
+
+// Per-kernel device times of un-captured steps (CUDA events on the handle's
+// stream around each launch).
+struct Prof {
+  cudaEvent_t a = nullptr, b = nullptr;
+  double stage_ms = 0.0, other_ms = 0.0;
+  int stage_launches = 0;
+};
+
+// Enqueue one time step on the handle's stream: [dt reduction], clock, then
+// per stage {ghost fill, fused stage kernel}.
+int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
+  auto mark = [&](cudaEvent_t e) -> int {
+    if (pf) FVM_CK(cudaEventRecord(e, h->stream));
+    return FVM_OK;
+  };
+  auto close = [&](bool stage) -> int {
+    if (!pf) return FVM_OK;
+    FVM_CK(cudaEventRecord(pf->b, h->stream));
+    FVM_CK(cudaEventSynchronize(pf->b));
+    float ms = 0.f;
+    FVM_CK(cudaEventElapsedTime(&ms, pf->a, pf->b));
+    if (stage) { pf->stage_ms += ms; pf->stage_launches += 1; }
+    else pf->other_ms += ms;
+    return FVM_OK;
+  };
+  int rc;
+  const bool state_dt = h->d.physics == FVM_NAVIER_STOKES;
+  if ((rc = mark(pf ? pf->a : nullptr))) return rc;
+  if (dt_mode == 0 && state_dt) {
+    cudaError_t e = h->f64 ? launch_dt_reduce<double>(h) : launch_dt_reduce<float>(h);
+    if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("dt reduction: ") + cudaGetErrorString(e));
+  }
+  const int cmode = dt_mode == 1 ? 1 : (state_dt ? 0 : 2);
+  clock_kernel<<<1, 1, 0, h->stream>>>(h->clk, cmode, h->max_inv_l2, h->const_rate, h->status);
+  FVM_CK(cudaGetLastError());
+  for (const StageDef& sd : stage_table(h->d.integrator)) {
+    cudaError_t e = launch_bc(h, sd.in, true);
+    if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
+    if ((rc = close(false))) return rc;
+    if ((rc = mark(pf ? pf->a : nullptr))) return rc;
+    e = h->f64 ? launch_stage<double>(h, sd, false) : launch_stage<float>(h, sd, false);
+    if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("stage kernel: ") + cudaGetErrorString(e));
+    if ((rc = close(true))) return rc;
+    if ((rc = mark(pf ? pf->a : nullptr))) return rc;
+  }
+  if (h->d.integrator == FVM_EULER_EXPLICIT) {
+    // Euler writes stage buffer 1; the state lives in buffer 0.
+    FVM_CK(cudaMemcpyAsync(h->U[0], h->U[1], h->lay.var_stride * h->nv * h->esz, cudaMemcpyDeviceToDevice,
+                           h->stream));
+  }
+  return close(false);
+}
+
+int ensure_graph(fvm_handle* h, int dt_mode) {
+  cudaGraphExec_t& ge = h->graph[dt_mode];
+  if (ge) return FVM_OK;
+  cudaGraph_t g;
+  {
+    StageDef sd{0, 1, MODE_RHS, ACC_NONE, 0, 0, 0};
+    FVM_CK(h->f64 ? launch_stage<double>(h, sd, true, true) : launch_stage<float>(h, sd, true, true));
+  }
+  FVM_CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_step(h, dt_mode, nullptr);
+  cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+  if (rc) return rc;
+  FVM_CK(ce);
+  ce = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  FVM_CK(ce);
+  return FVM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fvm_last_error(char* buf, int len) {
+  if (!buf || len <= 0) return FVM_E_INVALID;
+  std::snprintf(buf, (size_t)len, "%s", g_err.c_str());
+  return FVM_OK;
+}
+
+int fvm_create(const fvm_desc* desc, fvm_handle** out) {
+  if (!out) return fail(FVM_E_INVALID, "null output pointer");
+  *out = nullptr;
+  int rc = validate(desc);
+  if (rc) return rc;
+  fvm_handle* h = new fvm_handle();
+  h->d = *desc;
+  const fvm_desc& d = h->d;
+  h->nv = d.physics == FVM_NAVIER_STOKES ? 5 : (d.physics == FVM_HEAT ? 1 : 6);
+  h->f64 = d.precision == FVM_FP64;
+  h->esz = h->f64 ? 8 : 4;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, dev);
+  Layout& L = h->lay;
+  L.nx = d.nx1; L.ny = d.nx2; L.nz = d.nx3;
+  L.padx = h->f64 ? 1 : 3;
+  const long long row = (long long)L.nx + 2 + L.padx;
+  L.pitch = (row + 31) / 32 * 32;
+  L.plane = L.pitch * (L.ny + 2);
+  L.var_stride = (L.plane * (L.nz + 2) + 63) / 64 * 64;
+  h->zchunk = d.zchunk > 0 ? d.zchunk : 64;
+  auto cleanup = [&](int code) { fvm_destroy(h); return code; };
+#define FVM_CKC(x)                                                                                         \
+  do {                                                                                                     \
+    cudaError_t e_ = (x);                                                                                  \
+    if (e_ != cudaSuccess) return cleanup(fail(e_ == cudaErrorMemoryAllocation ? FVM_E_NOMEM : FVM_E_CUDA, \
+                                               std::string(#x) + ": " + cudaGetErrorString(e_)));          \
+  } while (0)
+  FVM_CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  const size_t state_bytes = (size_t)L.var_stride * h->nv * h->esz;
+  for (int b = 0; b < 3; ++b) {
+    FVM_CKC(cudaMalloc(&h->U[b], state_bytes));
+    FVM_CKC(cudaMemsetAsync(h->U[b], 0, state_bytes, h->stream));
+  }
+  h->device_bytes = 3 * (long long)state_bytes;
+  if (d.integrator == FVM_RK3 || d.integrator == FVM_RK4) {
+    FVM_CKC(cudaMalloc(&h->acc, state_bytes));
+    FVM_CKC(cudaMemsetAsync(h->acc, 0, state_bytes, h->stream));
+    h->device_bytes += state_bytes;
+  }
+  // metric tables
+  const HostMetric hm = build_metric(d);
+  const std::vector<double> packed = pack_metric(hm);
+  FVM_CKC(cudaMalloc(&h->met_f64, packed.size() * sizeof(double)));
+  FVM_CKC(cudaMemcpy(h->met_f64, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice));
+  h->md = metric_ptrs<double>(h->met_f64, d);
+  if (h->f64) {
+    h->met_real = h->met_f64;
+  } else {
+    std::vector<float> pf(packed.begin(), packed.end());
+    FVM_CKC(cudaMalloc(&h->met_real, pf.size() * sizeof(float)));
+    FVM_CKC(cudaMemcpy(h->met_real, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    h->mf = metric_ptrs<float>(static_cast<float*>(h->met_real), d);
+  }
+  // constant parts of the CFL step (navier_stokes.py:575, heat.py:331-338, maxwell.py:586-598)
+  double mx = 0.0, rmax = 0.0;
+  for (int k = 0; k < d.nx3; ++k)
+    for (int j = 0; j < d.nx2; ++j)
+      for (int i = 0; i < d.nx1; ++i) {
+        double Ls[3];
+        host_lengths(hm, d.coords, i, j, k, Ls);
+        const double s = (1.0 / (Ls[0] * Ls[0]) + 1.0 / (Ls[1] * Ls[1])) + 1.0 / (Ls[2] * Ls[2]);
+        mx = std::max(mx, s);
+        if (d.physics == FVM_MAXWELL) {
+          const double c = 1 / std::sqrt(d.params[0] * d.params[1]);
+          const double ml = std::max(std::fabs(-c), std::fabs(c));
+          rmax = std::max(rmax, std::max(std::max(ml / Ls[0], ml / Ls[1]), ml / Ls[2]));
+        }
+      }
+  h->max_inv_l2 = mx;
+  if (d.physics == FVM_HEAT) {
+    const double nu = d.params[2] / (d.params[0] * d.params[1]);
+    h->const_rate = 0.0 + (2 * nu) * mx;
+  } else if (d.physics == FVM_MAXWELL) {
+    const double chi = std::max(d.params[4], d.params[5]);
+    h->const_rate = rmax + (2.0 * chi) * mx;
+  }
+  FVM_CKC(cudaMalloc(&h->clk, sizeof(Clock)));
+  Clock c0{};
+  c0.t = 0.0;
+  c0.t_end = std::numeric_limits<double>::infinity();
+  c0.cfl = 0.4;
+  c0.active = 1;
+  FVM_CKC(cudaMemcpy(h->clk, &c0, sizeof(Clock), cudaMemcpyHostToDevice));
+  FVM_CKC(cudaMalloc(&h->status, sizeof(unsigned)));
+  FVM_CKC(cudaMemset(h->status, 0, sizeof(unsigned)));
+  FVM_CKC(cudaMalloc(&h->partials, sizeof(double) * 8 * 1024));
+  FVM_CKC(cudaMalloc(&h->totals_dev, sizeof(double) * 8));
+  h->stage_elems = (size_t)h->nv * (d.nx1 + 2) * (d.nx2 + 2) * (d.nx3 + 2);
+  FVM_CKC(cudaMalloc(&h->stage_dev, h->stage_elems * sizeof(double)));
+  FVM_CKC(cudaMallocHost(&h->stage_host, h->stage_elems * sizeof(double)));
+  h->device_bytes += h->stage_elems * sizeof(double);
+#undef FVM_CKC
+  const bool visc = d.physics == FVM_NAVIER_STOKES && d.params[1] != 0.0;
+  int rows;
+  if (d.physics == FVM_HEAT) rows = 8 + (d.reconstructor == FVM_PIECEWISE_CONSTANT ? 4 : 6);
+  else if (d.physics == FVM_MAXWELL) rows = 8 + 4;
+  else if (h->f64) rows = visc ? ns_tile_ty<double, true>() + 6 : ns_tile_ty<double, false>() + 4;
+  else rows = visc ? ns_tile_ty<float, true>() + 6 : ns_tile_ty<float, false>() + 4;
+  for (int b = 0; b < 3; ++b) {
+    rc = make_tmap(h, b, rows);
+    if (rc) { fvm_destroy(h); return rc; }
+  }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+    fvm_destroy(h);
+    return fail(FVM_E_CUDA, "initialisation failed");
+  }
+  *out = h;
+  return FVM_OK;
+}
+
+int fvm_destroy(fvm_handle* h) {
+  if (!h) return FVM_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto& g : h->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto& b : h->U)
+    if (b) cudaFree(b);
+  if (h->acc) cudaFree(h->acc);
+  if (h->met_real && h->met_real != h->met_f64) cudaFree(h->met_real);
+  if (h->met_f64) cudaFree(h->met_f64);
+  if (h->clk) cudaFree(h->clk);
+  if (h->status) cudaFree(h->status);
+  if (h->partials) cudaFree(h->partials);
+  if (h->totals_dev) cudaFree(h->totals_dev);
+  if (h->stage_dev) cudaFree(h->stage_dev);
+  if (h->stage_host) cudaFreeHost(h->stage_host);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return FVM_OK;
+}
+
+int fvm_info(const fvm_handle* h, int* nvars, long long* device_bytes) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  if (nvars) *nvars = h->nv;
+  if (device_bytes) *device_bytes = h->device_bytes;
+  return FVM_OK;
+}
+
+static int transpose(fvm_handle* h, bool to_device, int buf, bool interior) {
+  const fvm_desc& d = h->d;
+  const int m1 = interior ? d.nx1 : d.nx1 + 2, m2 = interior ? d.nx2 : d.nx2 + 2, m3 = interior ? d.nx3 : d.nx3 + 2;
+  const int off = interior ? 1 : 0;
+  dim3 grid((m3 + 31) / 32, (m1 + 31) / 32, m2 * h->nv), block(32, 8);
+  if (h->f64) {
+    if (to_device)
+      transpose_kernel<double, true><<<grid, block, 0, h->stream>>>(h->stage_dev, nullptr, nullptr,
+                                                                     static_cast<double*>(h->U[buf]), h->lay, m1, m2, m3, off);
+    else
+      transpose_kernel<double, false><<<grid, block, 0, h->stream>>>(nullptr, h->stage_dev,
+                                                                      static_cast<const double*>(h->U[buf]), nullptr,
+                                                                      h->lay, m1, m2, m3, off);
+  } else {
+    if (to_device)
+      transpose_kernel<float, true><<<grid, block, 0, h->stream>>>(h->stage_dev, nullptr, nullptr,
+                                                                    static_cast<float*>(h->U[buf]), h->lay, m1, m2, m3, off);
+    else
+      transpose_kernel<float, false><<<grid, block, 0, h->stream>>>(nullptr, h->stage_dev,
+                                                                     static_cast<const float*>(h->U[buf]), nullptr,
+                                                                     h->lay, m1, m2, m3, off);
+  }
+  FVM_CK(cudaGetLastError());
+  return FVM_OK;
+}
+
+int fvm_upload(fvm_handle* h, const double* host_state) {
+  if (!h || !host_state) return fail(FVM_E_INVALID, "null argument");
+  const size_t bytes = h->stage_elems * sizeof(double);
+  FVM_CK(cudaMemcpyAsync(h->stage_dev, host_state, bytes, cudaMemcpyHostToDevice, h->stream));
+  int rc = transpose(h, true, 0, false);
+  if (rc) return rc;
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+static void fill_edges_corners(double* f, int n1, int n2, int n3) {
+  // ghost edges/corners as averages of adjacent ghost faces (src/solver.py:39-61)
+  const int N[3] = {n1 + 2, n2 + 2, n3 + 2};
+  auto at = [&](int i, int j, int k) -> double& { return f[((long long)i * N[1] + j) * N[2] + k]; };
+  for (int a = 0; a < 3; ++a)
+    for (int b = a + 1; b < 3; ++b) {
+      const int c = 3 - a - b;
+      for (int ea = 0; ea < 2; ++ea)
+        for (int eb = 0; eb < 2; ++eb)
+          for (int t = 1; t <= N[c] - 2; ++t) {
+            int idx[3], p[3], q[3];
+            idx[a] = ea ? N[a] - 1 : 0;
+            idx[b] = eb ? N[b] - 1 : 0;
+            idx[c] = t;
+            for (int z = 0; z < 3; ++z) { p[z] = idx[z]; q[z] = idx[z]; }
+            p[a] = ea ? N[a] - 2 : 1;
+            q[b] = eb ? N[b] - 2 : 1;
+            at(idx[0], idx[1], idx[2]) = 0.5 * (at(p[0], p[1], p[2]) + at(q[0], q[1], q[2]));
+          }
+    }
+  for (int ci = 0; ci < 2; ++ci)
+    for (int cj = 0; cj < 2; ++cj)
+      for (int ck = 0; ck < 2; ++ck) {
+        const int i = ci ? N[0] - 1 : 0, j = cj ? N[1] - 1 : 0, k = ck ? N[2] - 1 : 0;
+        const int ii = ci ? N[0] - 2 : 1, jj = cj ? N[1] - 2 : 1, kk = ck ? N[2] - 2 : 1;
+        at(i, j, k) = (at(ii, j, k) + at(i, jj, k) + at(i, j, kk)) / 3.0;
+      }
+}
+
+int fvm_download(fvm_handle* h, double* host_state) {
+  if (!h || !host_state) return fail(FVM_E_INVALID, "null argument");
+  FVM_CK(launch_bc(h, 0, false));
+  int rc = transpose(h, false, 0, false);
+  if (rc) return rc;
+  FVM_CK(cudaMemcpyAsync(host_state, h->stage_dev, h->stage_elems * sizeof(double), cudaMemcpyDeviceToHost,
+                         h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  const size_t per = h->stage_elems / h->nv;
+  for (int q = 0; q < h->nv; ++q) fill_edges_corners(host_state + q * per, h->d.nx1, h->d.nx2, h->d.nx3);
+  return FVM_OK;
+}
+
+int fvm_residual(fvm_handle* h, double* host_rhs) {
+  if (!h || !host_rhs) return fail(FVM_E_INVALID, "null argument");
+  StageDef sd{0, 1, MODE_RHS, ACC_NONE, 0, 0, 0};
+  cudaError_t e = h->f64 ? launch_stage<double>(h, sd, true) : launch_stage<float>(h, sd, true);
+  if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("stage kernel: ") + cudaGetErrorString(e));
+  int rc = transpose(h, false, 1, true);
+  if (rc) return rc;
+  const size_t n = (size_t)h->nv * h->d.nx1 * h->d.nx2 * h->d.nx3;
+  FVM_CK(cudaMemcpyAsync(host_rhs, h->stage_dev, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+int fvm_set_time(fvm_handle* h, double t, double t_end, double cfl) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  if (!(cfl > 0.0)) return fail(FVM_E_INVALID, "CFL must be positive");
+  Clock c;
+  FVM_CK(cudaMemcpyAsync(&c, h->clk, sizeof(Clock), cudaMemcpyDeviceToHost, h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  c.t = t;
+  c.t_end = t_end;
+  c.cfl = cfl;
+  c.active = 1;
+  FVM_CK(cudaMemcpyAsync(h->clk, &c, sizeof(Clock), cudaMemcpyHostToDevice, h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+int fvm_set_dt(fvm_handle* h, double dt) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  if (!(dt > 0.0)) return fail(FVM_E_INVALID, "dt must be positive");
+  FVM_CK(cudaMemcpyAsync(&h->clk->dt_fixed, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+int fvm_get_time(fvm_handle* h, double* t, long long* steps, double* last_dt) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  Clock c;
+  FVM_CK(cudaMemcpyAsync(&c, h->clk, sizeof(Clock), cudaMemcpyDeviceToHost, h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  if (t) *t = c.t;
+  if (steps) *steps = c.steps;
+  if (last_dt) *last_dt = c.dt;
+  return FVM_OK;
+}
+
+int fvm_compute_dt(fvm_handle* h, double cfl, double* dt_out) {
+  if (!h || !dt_out) return fail(FVM_E_INVALID, "null argument");
+  if (!(cfl > 0.0)) return fail(FVM_E_INVALID, "CFL must be positive");
+  if (h->d.physics != FVM_NAVIER_STOKES) {
+    *dt_out = cfl / h->const_rate;
+    return FVM_OK;
+  }
+  cudaError_t e = h->f64 ? launch_dt_reduce<double>(h) : launch_dt_reduce<float>(h);
+  FVM_CK(e);
+  unsigned long long red[2];
+  FVM_CK(cudaMemcpyAsync(red, h->clk->red, sizeof(red), cudaMemcpyDeviceToHost, h->stream));
+  FVM_CK(cudaMemsetAsync(h->clk->red, 0, sizeof(red), h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  double rc, nu;
+  std::memcpy(&rc, &red[0], 8);
+  std::memcpy(&nu, &red[1], 8);
+  *dt_out = cfl / (rc + (2 * nu) * h->max_inv_l2);
+  return FVM_OK;
+}
+
+int fvm_step(fvm_handle* h, int n_steps, int dt_mode) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  if (dt_mode != 0 && dt_mode != 1) return fail(FVM_E_INVALID, "dt_mode must be 0 (CFL) or 1 (fixed)");
+  if (n_steps <= 0) return FVM_OK;
+  int rc = ensure_graph(h, dt_mode);
+  if (rc) return rc;
+  for (int s = 0; s < n_steps; ++s) FVM_CK(cudaGraphLaunch(h->graph[dt_mode], h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+int fvm_time_steps(fvm_handle* h, int n_steps, int dt_mode, double* ms) {
+  if (!h || !ms) return fail(FVM_E_INVALID, "null argument");
+  if (dt_mode != 0 && dt_mode != 1) return fail(FVM_E_INVALID, "dt_mode must be 0 (CFL) or 1 (fixed)");
+  int rc = ensure_graph(h, dt_mode);
+  if (rc) return rc;
+  cudaEvent_t a, b;
+  FVM_CK(cudaEventCreate(&a));
+  FVM_CK(cudaEventCreate(&b));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  FVM_CK(cudaEventRecord(a, h->stream));
+  for (int s = 0; s < n_steps; ++s) FVM_CK(cudaGraphLaunch(h->graph[dt_mode], h->stream));
+  FVM_CK(cudaEventRecord(b, h->stream));
+  FVM_CK(cudaEventSynchronize(b));
+  float t = 0.f;
+  FVM_CK(cudaEventElapsedTime(&t, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = t;
+  return FVM_OK;
+}
+
+int fvm_totals(fvm_handle* h, double* totals) {
+  if (!h || !totals) return fail(FVM_E_INVALID, "null argument");
+  const int nt = h->d.physics == FVM_MAXWELL ? h->nv + 1 : h->nv;
+  const int blocks = std::min(1024, h->nsm * 4);
+  const double emu = h->d.params[0], eep = h->d.params[1];
+#define FVM_TOT(R, C)                                                                                          \
+  totals_kernel<R, C><<<blocks, 256, 0, h->stream>>>(static_cast<const R*>(h->U[0]), h->lay, h->md, h->nv, nt, \
+                                                     emu, eep, h->partials)
+  if (h->f64) {
+    if (h->d.coords == FVM_CARTESIAN) FVM_TOT(double, COORD_CART);
+    else if (h->d.coords == FVM_CYLINDRICAL) FVM_TOT(double, COORD_CYL);
+    else FVM_TOT(double, COORD_SPH);
+  } else {
+    if (h->d.coords == FVM_CARTESIAN) FVM_TOT(float, COORD_CART);
+    else if (h->d.coords == FVM_CYLINDRICAL) FVM_TOT(float, COORD_CYL);
+    else FVM_TOT(float, COORD_SPH);
+  }
+#undef FVM_TOT
+  FVM_CK(cudaGetLastError());
+  totals_final_kernel<<<1, 32, 0, h->stream>>>(h->partials, blocks, nt, h->totals_dev);
+  FVM_CK(cudaGetLastError());
+  FVM_CK(cudaMemcpyAsync(totals, h->totals_dev, nt * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+int fvm_status(fvm_handle* h, unsigned* status) {
+  if (!h || !status) return fail(FVM_E_INVALID, "null argument");
+  FVM_CK(cudaMemcpyAsync(status, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+int fvm_clear_status(fvm_handle* h) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  FVM_CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_kernel_ms, double* other_kernel_ms,
+                      int* stage_launches) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  if (dt_mode != 0 && dt_mode != 1) return fail(FVM_E_INVALID, "dt_mode must be 0 (CFL) or 1 (fixed)");
+  Prof pf;
+  FVM_CK(cudaEventCreate(&pf.a));
+  FVM_CK(cudaEventCreate(&pf.b));
+  int rc = FVM_OK;
+  for (int s = 0; s < n_steps && !rc; ++s) rc = enqueue_step(h, dt_mode, &pf);
+  cudaEventDestroy(pf.a);
+  cudaEventDestroy(pf.b);
+  if (rc) return rc;
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  if (stage_kernel_ms) *stage_kernel_ms = pf.stage_ms;
+  if (other_kernel_ms) *other_kernel_ms = pf.other_ms;
+  if (stage_launches) *stage_launches = pf.stage_launches;
+  return FVM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,221 @@
+// Auxiliary kernels: ghost fill, layout transposes, CFL reduction, totals.
+#pragma once
+#include "fvm_common.cuh"
+
+namespace fvm {
+
+struct BcSpec {
+  signed char kind[6][6];  // [var][side]: 0 periodic, 1 neumann, 2 reflecting, 3 dirichlet
+  double value[6][6];
+};
+
+// Ghost face slabs of every variable (boundary_conditions.py:13-91 applied
+// per variable and side as in solver.py:30-37).  Edges and corners are never
+// read by the residual, so only the six face slabs are filled here.
+template <typename Real>
+__global__ void bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc, const int* active) {
+  if (active && !*active) return;
+  const long long nyz = (long long)L.ny * L.nz, nxz = (long long)L.nx * L.nz, nxy = (long long)L.nx * L.ny;
+  const long long per_var = 2 * (nyz + nxz + nxy);
+  const long long total = per_var * nv;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(t / per_var);
+    long long r = t % per_var;
+    int side, a, b;  // a, b: transverse interior indices (0-based)
+    if (r < 2 * nyz) { side = r < nyz ? 0 : 1; r %= nyz; a = (int)(r % L.ny); b = (int)(r / L.ny); }
+    else if ((r -= 2 * nyz) < 2 * nxz) { side = r < nxz ? 2 : 3; r %= nxz; a = (int)(r % L.nx); b = (int)(r / L.nx); }
+    else { r -= 2 * nxz; side = r < nxy ? 4 : 5; r %= nxy; a = (int)(r % L.nx); b = (int)(r / L.nx); }
+    const int kind = bc.kind[q][side];
+    const int axis = side >> 1, high = side & 1;
+    const int n = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
+    const int g = high ? n + 1 : 0;                       // ghost index along axis
+    const int inner = high ? n : 1;                       // adjacent interior
+    const int src = kind == 0 ? (high ? 1 : n) : inner;  // periodic: opposite layer
+    long long gi, si;
+    if (axis == 0) { gi = L.idx(q, b + 1, a + 1, g); si = L.idx(q, b + 1, a + 1, src); }
+    else if (axis == 1) { gi = L.idx(q, b + 1, g, a + 1); si = L.idx(q, b + 1, src, a + 1); }
+    else { gi = L.idx(q, g, b + 1, a + 1); si = L.idx(q, src, b + 1, a + 1); }
+    const Real v = u[si];
+    Real out;
+    if (kind == 2) out = -v;
+    else if (kind == 3) out = Real(2) * Real(bc.value[q][side]) - v;
+    else out = v;
+    u[gi] = out;
+  }
+}
+
+// Reference layout (C order, last axis fastest) <-> device layout (x1 fastest).
+// src/dst reference arrays have dims (nv, m1, m2, m3) and map to ghosted device
+// indices g = m + off.  32x32 shared-memory tiles over (x1, x3) per (var, x2).
+template <typename Real, bool TO_DEVICE>
+__global__ void transpose_kernel(const double* __restrict__ hsrc, double* __restrict__ hdst,
+                                 const Real* __restrict__ dsrc, Real* __restrict__ ddst, Layout L, int m1,
+                                 int m2, int m3, int off) {
+  __shared__ double tile[32][33];
+  const int q = blockIdx.z / m2, j = blockIdx.z % m2;
+  const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  if (TO_DEVICE) {
+    for (int m = ty; m < 32; m += 8) {
+      const int i = i0 + m, k = k0 + tx;
+      if (i < m1 && k < m3) tile[m][tx] = hsrc[(((long long)q * m1 + i) * m2 + j) * m3 + k];
+    }
+    __syncthreads();
+    for (int m = ty; m < 32; m += 8) {
+      const int k = k0 + m, i = i0 + tx;
+      if (i < m1 && k < m3) ddst[L.idx(q, k + off, j + off, i + off)] = Real(tile[tx][m]);
+    }
+  } else {
+    for (int m = ty; m < 32; m += 8) {
+      const int k = k0 + m, i = i0 + tx;
+      if (i < m1 && k < m3) tile[tx][m] = double(dsrc[L.idx(q, k + off, j + off, i + off)]);
+    }
+    __syncthreads();
+    for (int m = ty; m < 32; m += 8) {
+      const int i = i0 + m, k = k0 + tx;
+      if (i < m1 && k < m3) hdst[(((long long)q * m1 + i) * m2 + j) * m3 + k] = tile[m][tx];
+    }
+  }
+}
+
+// Device-resident time-loop scalars.
+struct Clock {
+  double t, t_end, dt, cfl, dt_fixed;
+  long long steps;
+  int active;
+  unsigned long long red[2];  // running maxima (bit patterns of non-negative doubles)
+};
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
+  atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+// CFL rates of the Navier-Stokes state (navier_stokes.py:512-585) in float64:
+// red[0] = max_cells max_d max_w |v_d + kappa_w| / L_d, red[1] = max mu/rho.
+template <typename Real, int COORD>
+__global__ void ns_dt_reduce_kernel(const Real* __restrict__ u, Layout L, Metric<double> m, double gam, double mu,
+                                    Clock* clk, unsigned* status) {
+  if (!clk->active) return;
+  __shared__ double s_rc[32], s_nu[32];
+  double rc = 0.0, nu = 0.0;
+  unsigned bad = 0;
+  const long long n = (long long)L.nx * L.ny * L.nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % L.nx), j = (int)((c / L.nx) % L.ny), k = (int)(c / ((long long)L.nx * L.ny));
+    const long long g = L.idx(0, k + 1, j + 1, i + 1);
+    const double rho = double(u[g]);
+    const double v0 = double(u[g + L.var_stride]) / rho, v1 = double(u[g + 2 * L.var_stride]) / rho,
+                 v2 = double(u[g + 3 * L.var_stride]) / rho;
+    const double E = double(u[g + 4 * L.var_stride]) / rho;
+    const double P = ((gam - 1.0) * rho) * (E - (((v0 * v0) + (v1 * v1)) + (v2 * v2)) / 2.0);
+    const double cs = sqrt((gam * P) / rho);
+    if (!(rho > 0.0)) bad |= ST_DENSITY;
+    if (!(P > 0.0)) bad |= ST_PRESSURE;
+    const double vv[3] = {v0, v1, v2};
+    double ml[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) ml[d] = fmax(fmax(fabs(vv[d] + 0.0), fabs(vv[d] + (-cs))), fabs(vv[d] + cs));
+    const double l1 = Geo<double, COORD>::L1(m, i, j, k), l2 = Geo<double, COORD>::L2(m, i, j, k),
+                 l3 = Geo<double, COORD>::L3(m, i, j, k);
+    const double r = fmax(fmax(ml[0] / l1, ml[1] / l2), ml[2] / l3);
+    const double nl = mu / rho;
+    if (!(r >= 0.0) || !(nl >= 0.0)) bad |= ST_NONFINITE;
+    rc = fmax(rc, r);
+    nu = fmax(nu, nl);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    rc = fmax(rc, __shfl_xor_sync(0xffffffffu, rc, o));
+    nu = fmax(nu, __shfl_xor_sync(0xffffffffu, nu, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { s_rc[w] = rc; s_nu[w] = nu; }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    rc = l < nw ? s_rc[l] : 0.0;
+    nu = l < nw ? s_nu[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      rc = fmax(rc, __shfl_xor_sync(0xffffffffu, rc, o));
+      nu = fmax(nu, __shfl_xor_sync(0xffffffffu, nu, o));
+    }
+    if (l == 0) {
+      atomic_max_pos(&clk->red[0], rc);
+      atomic_max_pos(&clk->red[1], nu);
+    }
+  }
+  if (bad) atomicOr(status, bad);
+}
+
+// One thread: close the step's clock.  mode 0: dt from the reduced NS rates,
+// mode 1: fixed dt, mode 2: dt = cfl / const_rate (state-independent heat and
+// Maxwell steps).  `max_inv_l2` = max over cells of sum_d 1/L_d^2.
+__global__ void clock_kernel(Clock* clk, int mode, double max_inv_l2, double const_rate, unsigned* status) {
+  clk->active = clk->t <= clk->t_end ? 1 : 0;
+  double dt;
+  if (mode == 0) {
+    const double rc = __longlong_as_double((long long)clk->red[0]);
+    const double nu = __longlong_as_double((long long)clk->red[1]);
+    clk->red[0] = 0ull;
+    clk->red[1] = 0ull;
+    const double rd = (2 * nu) * max_inv_l2;
+    dt = clk->cfl / (rc + rd);
+  } else if (mode == 1) {
+    dt = clk->dt_fixed;
+  } else {
+    dt = clk->cfl / const_rate;
+  }
+  if (!clk->active) return;
+  if (!(dt > 0.0) || !isfinite(dt)) atomicOr(status, ST_DT);
+  clk->dt = dt;
+  clk->t = clk->t + dt;
+  clk->steps = clk->steps + 1;
+}
+
+// Conserved totals with Neumaier compensation: per-thread, then per-block
+// (fixed order), then a single-thread pass over the block partials.
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double x) {
+  const double t = s + x;
+  if (fabs(s) >= fabs(x)) c += (s - t) + x;
+  else c += (x - t) + s;
+  s = t;
+}
+
+template <typename Real, int COORD>
+__global__ void totals_kernel(const Real* __restrict__ u, Layout L, Metric<double> m, int nv, int nt,
+                              double em_mu, double em_ep, double* __restrict__ partials) {
+  // nt totals: the nv conserved sums, plus (Maxwell) EM energy when nt == nv + 1
+  __shared__ double ss[256][8];
+  double s[8], c[8];
+  for (int q = 0; q < 8; ++q) { s[q] = 0.0; c[q] = 0.0; }
+  const long long n = (long long)L.nx * L.ny * L.nz;
+  for (long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x; cell < n;
+       cell += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(cell % L.nx), j = (int)((cell / L.nx) % L.ny), k = (int)(cell / ((long long)L.nx * L.ny));
+    const double V = Geo<double, COORD>::V(m, i, j, k);
+    const long long g = L.idx(0, k + 1, j + 1, i + 1);
+    double em = 0.0;
+    for (int q = 0; q < nv; ++q) {
+      const double x = double(u[g + q * L.var_stride]);
+      neumaier_add(s[q], c[q], x * V);
+      if (nt > nv) em += q < 3 ? (x * x) / em_mu : (x * x) / em_ep;
+    }
+    if (nt > nv) neumaier_add(s[nv], c[nv], 0.5 * em * V);
+  }
+  for (int q = 0; q < nt; ++q) ss[threadIdx.x][q] = s[q] + c[q];
+  __syncthreads();
+  if (threadIdx.x < nt) {
+    double bs = 0.0, bc = 0.0;
+    for (int t = 0; t < (int)blockDim.x; ++t) neumaier_add(bs, bc, ss[t][threadIdx.x]);
+    partials[blockIdx.x * 8 + threadIdx.x] = bs + bc;
+  }
+}
+
+__global__ void totals_final_kernel(const double* __restrict__ partials, int nblocks, int nt, double* out) {
+  if (threadIdx.x >= nt) return;
+  double s = 0.0, c = 0.0;
+  for (int b = 0; b < nblocks; ++b) neumaier_add(s, c, partials[b * 8 + threadIdx.x]);
+  out[threadIdx.x] = s + c;
+}
+
+}  // namespace fvm

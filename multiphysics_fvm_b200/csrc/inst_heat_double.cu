@@ -1,0 +1,5 @@
+// Explicit instantiation: heat stage kernels, double, all limiters and coordinates.
+#include "launch.cuh"
+namespace fvm {
+template cudaError_t launch_heat<double>(int, int, const CUtensorMap&, const HeatParams<double>&, cudaStream_t, int);
+}

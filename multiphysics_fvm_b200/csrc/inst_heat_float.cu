@@ -1,0 +1,5 @@
+// Explicit instantiation: heat stage kernels, float, all limiters and coordinates.
+#include "launch.cuh"
+namespace fvm {
+template cudaError_t launch_heat<float>(int, int, const CUtensorMap&, const HeatParams<float>&, cudaStream_t, int);
+}

@@ -1,0 +1,6 @@
+// Explicit instantiation: Maxwell stage kernels, double, COORD_SPH.
+#include "launch.cuh"
+namespace fvm {
+template cudaError_t launch_maxwell_coord<double, COORD_SPH>(int, int, const CUtensorMap&, const MaxwellParams<double>&,
+                                                          cudaStream_t, int);
+}

@@ -1,0 +1,6 @@
+// Explicit instantiation: Maxwell stage kernels, float, COORD_SPH.
+#include "launch.cuh"
+namespace fvm {
+template cudaError_t launch_maxwell_coord<float, COORD_SPH>(int, int, const CUtensorMap&, const MaxwellParams<float>&,
+                                                          cudaStream_t, int);
+}

@@ -1,0 +1,181 @@
+// Launch helpers for the fused stage kernels: persistent grids sized from the
+// occupancy of each instantiation, runtime dispatch over the scheme enums.
+#pragma once
+#include <type_traits>
+#include "stage_ns.cuh"
+#include "stage_heat.cuh"
+#include "stage_maxwell.cuh"
+
+namespace fvm {
+
+// Tile rows of the Navier-Stokes kernel and the blocks per SM it is built
+// for: float32 viscous 6 rows (2 blocks of 256 threads, ~109 KB each),
+// float32 inviscid 8 rows (2 blocks), float64 viscous 4 rows, inviscid 8.
+template <typename Real, bool VISC>
+constexpr int ns_tile_ty() { return std::is_same<Real, double>::value ? (VISC ? 4 : 8) : (VISC ? 6 : 8); }
+template <typename Real, bool VISC>
+constexpr int ns_min_blocks() { return std::is_same<Real, double>::value ? 1 : 2; }
+
+template <typename K>
+static cudaError_t prepare_kernel(K kern, int threads, int bytes, int* blocks_per_sm) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, threads, bytes);
+  if (e != cudaSuccess) return e;
+  if (*blocks_per_sm < 1) return cudaErrorInvalidConfiguration;
+  return cudaSuccess;
+}
+
+// nsm < 0: only set the kernel's shared-memory attribute and query its
+// occupancy (done once, outside any stream capture).
+template <typename Real, int LIM, int RIEM, int COORD, bool VISC>
+cudaError_t launch_ns_one(const CUtensorMap& map, NsParams<Real> p, cudaStream_t s, int nsm) {
+  constexpr int TY = ns_tile_ty<Real, VISC>();
+  using C = NsCfg<Real, VISC, TY>;
+  auto kern = ns_stage_kernel<Real, LIM, RIEM, COORD, VISC, TY, ns_min_blocks<Real, VISC>()>;
+  static int bps = 0;
+  if (bps == 0 || nsm < 0) {
+    cudaError_t e = prepare_kernel(kern, C::NT, C::BYTES, &bps);
+    if (e != cudaSuccess) return e;
+  }
+  if (nsm < 0) return cudaSuccess;
+  p.ntx = (p.lay.nx + C::TX - 1) / C::TX;
+  p.nty = (p.lay.ny + TY - 1) / TY;
+  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
+  const long long ntiles = (long long)p.ntx * p.nty * p.nzc;
+  const int grid = (int)(ntiles < (long long)bps * nsm ? ntiles : (long long)bps * nsm);
+  kern<<<grid, C::NT, C::BYTES, s>>>(map, p);
+  return cudaGetLastError();
+}
+
+template <typename Real, int COORD>
+cudaError_t launch_ns_coord(int lim, int riem, bool visc, const CUtensorMap& map, const NsParams<Real>& p,
+                            cudaStream_t s, int nsm) {
+#define FVM_NS_CASE(L, R)                                                          \
+  if (lim == L && riem == R)                                                       \
+    return visc ? launch_ns_one<Real, L, R, COORD, true>(map, p, s, nsm)           \
+                : launch_ns_one<Real, L, R, COORD, false>(map, p, s, nsm);
+  FVM_NS_CASE(LIM_PC, RIEM_RUSANOV)
+  FVM_NS_CASE(LIM_PC, RIEM_HLL)
+  FVM_NS_CASE(LIM_MINMOD, RIEM_RUSANOV)
+  FVM_NS_CASE(LIM_MINMOD, RIEM_HLL)
+  FVM_NS_CASE(LIM_MC, RIEM_RUSANOV)
+  FVM_NS_CASE(LIM_MC, RIEM_HLL)
+  FVM_NS_CASE(LIM_VANLEER, RIEM_RUSANOV)
+  FVM_NS_CASE(LIM_VANLEER, RIEM_HLL)
+#undef FVM_NS_CASE
+  return cudaErrorInvalidValue;
+}
+
+// Declarations of the per-(precision, coordinate) instantiations.
+#define FVM_DECLARE_NS(REAL, COORD)                                                                      \
+  extern template cudaError_t launch_ns_coord<REAL, COORD>(int, int, bool, const CUtensorMap&,          \
+                                                          const NsParams<REAL>&, cudaStream_t, int);
+FVM_DECLARE_NS(float, COORD_CART)
+FVM_DECLARE_NS(float, COORD_CYL)
+FVM_DECLARE_NS(float, COORD_SPH)
+FVM_DECLARE_NS(double, COORD_CART)
+FVM_DECLARE_NS(double, COORD_CYL)
+FVM_DECLARE_NS(double, COORD_SPH)
+
+template <typename Real>
+cudaError_t launch_ns(int lim, int riem, int coord, bool visc, const CUtensorMap& map, const NsParams<Real>& p,
+                      cudaStream_t s, int nsm) {
+  if (coord == COORD_CART) return launch_ns_coord<Real, COORD_CART>(lim, riem, visc, map, p, s, nsm);
+  if (coord == COORD_CYL) return launch_ns_coord<Real, COORD_CYL>(lim, riem, visc, map, p, s, nsm);
+  return launch_ns_coord<Real, COORD_SPH>(lim, riem, visc, map, p, s, nsm);
+}
+
+// ---------------------------------------------------------------- heat ----
+template <typename Real, int LIM, int COORD>
+cudaError_t launch_heat_one(const CUtensorMap& map, HeatParams<Real> p, cudaStream_t s, int nsm) {
+  constexpr int TY = 8;
+  using C = HeatCfg<Real, LIM, TY>;
+  auto kern = heat_stage_kernel<Real, LIM, COORD, TY>;
+  static int bps = 0;
+  if (bps == 0 || nsm < 0) {
+    cudaError_t e = prepare_kernel(kern, C::NT, C::BYTES, &bps);
+    if (e != cudaSuccess) return e;
+  }
+  if (nsm < 0) return cudaSuccess;
+  p.ntx = (p.lay.nx + C::TX - 1) / C::TX;
+  p.nty = (p.lay.ny + TY - 1) / TY;
+  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
+  const long long ntiles = (long long)p.ntx * p.nty * p.nzc;
+  const int grid = (int)(ntiles < (long long)bps * nsm ? ntiles : (long long)bps * nsm);
+  kern<<<grid, C::NT, C::BYTES, s>>>(map, p);
+  return cudaGetLastError();
+}
+
+template <typename Real>
+cudaError_t launch_heat(int lim, int coord, const CUtensorMap& map, const HeatParams<Real>& p, cudaStream_t s,
+                        int nsm) {
+#define FVM_HEAT_CASE(L)                                                                       \
+  if (lim == L) {                                                                              \
+    if (coord == COORD_CART) return launch_heat_one<Real, L, COORD_CART>(map, p, s, nsm);     \
+    if (coord == COORD_CYL) return launch_heat_one<Real, L, COORD_CYL>(map, p, s, nsm);       \
+    return launch_heat_one<Real, L, COORD_SPH>(map, p, s, nsm);                               \
+  }
+  FVM_HEAT_CASE(LIM_PC)
+  FVM_HEAT_CASE(LIM_MINMOD)
+  FVM_HEAT_CASE(LIM_MC)
+  FVM_HEAT_CASE(LIM_VANLEER)
+#undef FVM_HEAT_CASE
+  return cudaErrorInvalidValue;
+}
+extern template cudaError_t launch_heat<float>(int, int, const CUtensorMap&, const HeatParams<float>&, cudaStream_t, int);
+extern template cudaError_t launch_heat<double>(int, int, const CUtensorMap&, const HeatParams<double>&, cudaStream_t, int);
+
+// ------------------------------------------------------------- maxwell ----
+template <typename Real, int LIM, int RIEM, int COORD>
+cudaError_t launch_maxwell_one(const CUtensorMap& map, MaxwellParams<Real> p, cudaStream_t s, int nsm) {
+  constexpr int TY = 8;
+  using C = MaxwellCfg<Real, TY>;
+  auto kern = maxwell_stage_kernel<Real, LIM, RIEM, COORD, TY>;
+  static int bps = 0;
+  if (bps == 0 || nsm < 0) {
+    cudaError_t e = prepare_kernel(kern, C::NT, C::BYTES, &bps);
+    if (e != cudaSuccess) return e;
+  }
+  if (nsm < 0) return cudaSuccess;
+  p.ntx = (p.lay.nx + C::TX - 1) / C::TX;
+  p.nty = (p.lay.ny + TY - 1) / TY;
+  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
+  const long long ntiles = (long long)p.ntx * p.nty * p.nzc;
+  const int grid = (int)(ntiles < (long long)bps * nsm ? ntiles : (long long)bps * nsm);
+  kern<<<grid, C::NT, C::BYTES, s>>>(map, p);
+  return cudaGetLastError();
+}
+
+template <typename Real, int COORD>
+cudaError_t launch_maxwell_coord(int lim, int riem, const CUtensorMap& map, const MaxwellParams<Real>& p,
+                                 cudaStream_t s, int nsm) {
+#define FVM_MX_CASE(L)                                                                           \
+  if (lim == L) return riem == RIEM_HLL ? launch_maxwell_one<Real, L, RIEM_HLL, COORD>(map, p, s, nsm) \
+                                        : launch_maxwell_one<Real, L, RIEM_RUSANOV, COORD>(map, p, s, nsm);
+  FVM_MX_CASE(LIM_PC)
+  FVM_MX_CASE(LIM_MINMOD)
+  FVM_MX_CASE(LIM_MC)
+  FVM_MX_CASE(LIM_VANLEER)
+#undef FVM_MX_CASE
+  return cudaErrorInvalidValue;
+}
+#define FVM_DECLARE_MX(REAL, COORD)                                                                      \
+  extern template cudaError_t launch_maxwell_coord<REAL, COORD>(int, int, const CUtensorMap&,           \
+                                                               const MaxwellParams<REAL>&, cudaStream_t, int);
+FVM_DECLARE_MX(float, COORD_CART)
+FVM_DECLARE_MX(float, COORD_CYL)
+FVM_DECLARE_MX(float, COORD_SPH)
+FVM_DECLARE_MX(double, COORD_CART)
+FVM_DECLARE_MX(double, COORD_CYL)
+FVM_DECLARE_MX(double, COORD_SPH)
+
+template <typename Real>
+cudaError_t launch_maxwell(int lim, int riem, int coord, const CUtensorMap& map, const MaxwellParams<Real>& p,
+                           cudaStream_t s, int nsm) {
+  if (coord == COORD_CART) return launch_maxwell_coord<Real, COORD_CART>(lim, riem, map, p, s, nsm);
+  if (coord == COORD_CYL) return launch_maxwell_coord<Real, COORD_CYL>(lim, riem, map, p, s, nsm);
+  return launch_maxwell_coord<Real, COORD_SPH>(lim, riem, map, p, s, nsm);
+}
+
+}  // namespace fvm

@@ -1,0 +1,247 @@
+// Fused heat stage kernel: residual (heat.py:354-473) + Runge-Kutta stage.
+//
+// rhs = -sum_faces (phi_a,L + phi_a,R)/2 * S / V + q with phi = -k grad T,
+// T = rho_cp_T / (rho cp), phi zero-padded in the ghosts (heat.py:40-102) and
+// phi_a reconstructed along axis a (piecewise constant or MUSCL).
+// Same z-march skeleton as the Navier-Stokes kernel: at step K the TMA ring
+// receives plane K+HH; T of that plane, phi of plane K+HH-1, x3 slopes of
+// phi_3 at K+1 and the x3 face flux at K+1/2 follow; then the x1/x2 fluxes
+// of plane K go through shared memory.  HH = 3 for MUSCL (phi at K+2 needs T
+// at K+3), 2 for piecewise constant.
+#pragma once
+#include "stage_ns.cuh"
+
+namespace fvm {
+
+template <typename Real>
+struct HeatParams {
+  Layout lay;
+  Metric<Real> met;
+  const Real* u0;
+  Real* out;
+  Real* acc;
+  const double* dt;
+  const int* active;
+  StageCoef coef;
+  double rho_cp, k, q;
+  unsigned* status;
+  int zchunk, ntx, nty, nzc;
+};
+
+template <typename Real, int LIM, int TY>
+struct HeatCfg {
+  static constexpr int TX = 32;
+  static constexpr int NT = TX * (TY + 2);
+  static constexpr int HH = LIM == LIM_PC ? 2 : 3;
+  static constexpr int W = 40;
+  static constexpr int ROWS = TY + 2 * HH;
+  static constexpr int PL = ROWS * W;
+  static constexpr int NSLOT = HH + 2;
+  static constexpr int SLOT = round_up(PL * (int)sizeof(Real), 128) / (int)sizeof(Real);
+  static constexpr int XB = cmax(TY * (TX + 2), (TY + 2) * TX);
+  static constexpr int FB = cmax(TY * (TX + 1), (TY + 1) * TX);
+  static constexpr int OFF_U = 0;
+  static constexpr int OFF_T = OFF_U + NSLOT * SLOT;
+  static constexpr int OFF_PHI = OFF_T + 3 * PL;
+  static constexpr int OFF_FL = OFF_PHI + 3 * 3 * PL;
+  static constexpr int OFF_FR = OFF_FL + XB;
+  static constexpr int OFF_FB = OFF_FR + XB;
+  static constexpr int END = OFF_FB + FB;
+  static constexpr int BYTES = round_up(END * (int)sizeof(Real), 16) + NSLOT * 8;
+  static constexpr unsigned TX_BYTES = PL * sizeof(Real);
+};
+
+template <typename Real, int LIM, int COORD, int TY>
+__global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
+    heat_stage_kernel(const __grid_constant__ CUtensorMap tmap, const HeatParams<Real> p) {
+  using C = HeatCfg<Real, LIM, TY>;
+  using G = Geo<Real, COORD>;
+  constexpr int TX = C::TX, NT = C::NT, W = C::W, PL = C::PL, HH = C::HH;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Real* sm = reinterpret_cast<Real*>(smem_raw);
+  Real* uring = sm + C::OFF_U;
+  Real* tring = sm + C::OFF_T;
+  Real* phring = sm + C::OFF_PHI;
+  Real* fL = sm + C::OFF_FL;
+  Real* fR = sm + C::OFF_FR;
+  Real* fb = sm + C::OFF_FB;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (C::BYTES - C::NSLOT * 8));
+  if (p.active && !*p.active) return;
+  if (smem_u32(smem_raw) & 127u) {
+    if (threadIdx.x == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+    return;
+  }
+  const int tid = threadIdx.x;
+  const Layout& L = p.lay;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const Real rcp = Real(p.rho_cp), kk = Real(p.k), qsrc = Real(p.q);
+  const Real dt = Real(*p.dt);
+  if (tid == 0) {
+    tma_prefetch_desc(&tmap);
+    for (int s = 0; s < C::NSLOT; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  unsigned phase_bits = 0, pending = 0;
+  auto U = [&](int pl, int r, int c) -> Real& { return uring[pmod(pl, C::NSLOT) * C::SLOT + r * W + c]; };
+  auto T = [&](int pl, int r, int c) -> Real& { return tring[pmod(pl, 3) * PL + r * W + c]; };
+  auto Ph = [&](int pl, int a, int r, int c) -> Real& { return phring[(pmod(pl, 3) * 3 + a) * PL + r * W + c]; };
+
+  const bool is_out = tid < TX * TY;
+  const int otx = tid % TX, oty = tid / TX;
+  const int ntiles = p.ntx * p.nty * p.nzc;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int x0 = (tile % p.ntx) * TX, y0 = ((tile / p.ntx) % p.nty) * TY;
+    const int Z0 = 1 + (tile / (p.ntx * p.nty)) * p.zchunk;
+    const int Zl = min(Z0 + p.zchunk - 1, nz);
+    const int Pfirst = Z0 - HH, Plast = Zl + HH, Kfirst = Z0 - 2 * HH;
+    const int oi = x0 + otx, oj = y0 + oty;
+    const bool out_valid = is_out && oi < nx && oj < ny;
+    Real zs = Real(0), Fzp = Real(0), Fzn = Real(0);
+    const Real S3c = out_valid ? G::S3(p.met, oi, oj) : Real(0);
+    auto issue = [&](int pl) {
+      const int s = pmod(pl, C::NSLOT);
+      pending |= 1u << s;
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&bars[s], C::TX_BYTES);
+      tma_load_4d(&uring[s * C::SLOT], &tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
+    };
+    if (tid == 0) issue(Pfirst);
+    for (int K = Kfirst; K <= Zl; ++K) {
+      if (tid == 0 && K + HH + 1 <= Plast) issue(K + HH + 1);
+      {
+        const int s = pmod(K + HH, C::NSLOT);
+        const bool got = mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 2000000000ull);
+        if (!__syncthreads_and(got)) {
+          if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+          ok = false;
+          break;
+        }
+        phase_bits ^= 1u << s;
+        pending &= ~(1u << s);
+      }
+      // T on the newest plane (heat.py:74)
+      {
+        const int pl = K + HH;
+        for (int it = tid; it < C::ROWS * (TX + 6); it += NT) {
+          const int r = it / (TX + 6), c = 1 + it % (TX + 6);
+          T(pl, r, c) = U(pl, r, c) / rcp;
+        }
+      }
+      __syncthreads();
+      // phi = -k grad T on plane K+HH-1 (heat.py:85-95), zero on ghosts, over
+      // the tile plus PH = HH-1 cells (what the x1/x2 face states read)
+      if (K >= Z0 - 2 * HH + 2) {
+        constexpr int PH = HH - 1;
+        const int pl = K + HH - 1, k = pl - 1;
+        const bool zg = k < 0 || k >= nz;
+        for (int it = tid; it < (TY + 2 * PH) * (TX + 2 * PH); it += NT) {
+          const int r = HH - PH + it / (TX + 2 * PH), c = 4 - PH + it % (TX + 2 * PH);
+          const int i = x0 + c - 4, j = y0 + r - HH;
+          Real f0 = Real(0), f1 = Real(0), f2 = Real(0);
+          if (!(zg || i < 0 || i >= nx || j < 0 || j >= ny)) {
+            const Real l1 = G::L1(p.met, i, j, k), l2 = G::L2(p.met, i, j, k), l3 = G::L3(p.met, i, j, k);
+            f0 = (-kk) * ((T(pl, r, c + 1) - T(pl, r, c - 1)) / (Real(2) * l1));
+            f1 = (-kk) * ((T(pl, r + 1, c) - T(pl, r - 1, c)) / (Real(2) * l2));
+            f2 = (-kk) * ((T(pl + 1, r, c) - T(pl - 1, r, c)) / (Real(2) * l3));
+          }
+          Ph(pl, 0, r, c) = f0;
+          Ph(pl, 1, r, c) = f1;
+          Ph(pl, 2, r, c) = f2;
+        }
+      }
+      __syncthreads();
+      // x3: slope of phi_3 at K+1 (MUSCL) and the face flux at K+1/2
+      if (K >= Z0 - 2 && is_out) {
+        const int r = oty + HH, c = otx + 4;
+        Real zn = Real(0);
+        if constexpr (LIM != LIM_PC) {
+          const bool ghost = (K + 1 <= 0 || K + 1 >= nz + 1);
+          if (!ghost && out_valid)
+            zn = muscl_slope<LIM>(Ph(K, 2, r, c), Ph(K + 1, 2, r, c), Ph(K + 2, 2, r, c), G::L3(p.met, oi, oj, K));
+        }
+        if (K >= Z0 - 1) {
+          const Real fl = Ph(K, 2, r, c) + zs / Real(2);
+          const Real fr = Ph(K + 1, 2, r, c) - zn / Real(2);
+          Fzp = Fzn;
+          Fzn = (Real(0) + (fl + fr) / Real(2)) * S3c;
+        }
+        zs = zn;
+      }
+      if (K < Z0) { __syncthreads(); continue; }
+      const int kK = K - 1;
+      // x1 faces of plane K
+      for (int it = tid; it < TY * (TX + 2); it += NT) {
+        const int ty = it / (TX + 2), tx = it % (TX + 2) - 1;
+        const int r = ty + HH, c = tx + 4, i = x0 + tx, j = y0 + ty;
+        const Real f0 = Ph(K, 0, r, c);
+        Real s = Real(0);
+        if constexpr (LIM != LIM_PC) {
+          if (i >= 0 && i < nx && j < ny) s = muscl_slope<LIM>(Ph(K, 0, r, c - 1), f0, Ph(K, 0, r, c + 1), G::L1(p.met, i, j, kK));
+        }
+        const int o = ty * (TX + 2) + tx + 1;
+        fL[o] = f0 + s / Real(2);
+        fR[o] = f0 - s / Real(2);
+      }
+      __syncthreads();
+      for (int it = tid; it < TY * (TX + 1); it += NT) {
+        const int ty = it / (TX + 1), fx = it % (TX + 1), fi = x0 + fx, j = y0 + ty;
+        Real F = Real(0);
+        if (fi <= nx && j < ny) {
+          const int o = ty * (TX + 2) + fx;
+          F = (Real(0) + (fL[o] + fR[o + 1]) / Real(2)) * G::S1(p.met, fi, j, kK);
+        }
+        fb[ty * (TX + 1) + fx] = F;
+      }
+      __syncthreads();
+      Real Fxm = Real(0), Fxp = Real(0);
+      if (is_out) { Fxm = fb[oty * (TX + 1) + otx]; Fxp = fb[oty * (TX + 1) + otx + 1]; }
+      // x2 faces
+      for (int it = tid; it < (TY + 2) * TX; it += NT) {
+        const int ty = it / TX - 1, tx = it % TX;
+        const int r = ty + HH, c = tx + 4, i = x0 + tx, j = y0 + ty;
+        const Real f0 = Ph(K, 1, r, c);
+        Real s = Real(0);
+        if constexpr (LIM != LIM_PC) {
+          if (i < nx && j >= 0 && j < ny) s = muscl_slope<LIM>(Ph(K, 1, r - 1, c), f0, Ph(K, 1, r + 1, c), G::L2(p.met, i, j, kK));
+        }
+        const int o = (ty + 1) * TX + tx;
+        fL[o] = f0 + s / Real(2);
+        fR[o] = f0 - s / Real(2);
+      }
+      __syncthreads();
+      for (int it = tid; it < (TY + 1) * TX; it += NT) {
+        const int fy = it / TX, tx = it % TX, fj = y0 + fy, i = x0 + tx;
+        Real F = Real(0);
+        if (fj <= ny && i < nx) {
+          const int o = fy * TX + tx;
+          F = (Real(0) + (fL[o] + fR[o + TX]) / Real(2)) * G::S2(p.met, i, fj, kK);
+        }
+        fb[fy * TX + tx] = F;
+      }
+      __syncthreads();
+      if (out_valid) {
+        const Real Fym = fb[oty * TX + otx], Fyp = fb[(oty + 1) * TX + otx];
+        const Real sum = ((((Fxp - Fxm) + Fyp) - Fym) + Fzn) - Fzp;
+        const Real k = (-sum) / G::V(p.met, oi, oj, kK) + qsrc;
+        const long long gi = L.idx(0, K, oj + 1, oi + 1);
+        const Real ucur = U(K, oty + HH, otx + 4);
+        Real u0v = Real(0), accv = Real(0);
+        if (p.coef.mode >= MODE_AXPY) u0v = p.u0[gi];
+        if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
+        const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
+        p.out[gi] = o;
+        if (p.coef.accmode == ACC_SET) p.acc[gi] = k;
+        else if (p.coef.accmode == ACC_ADD) p.acc[gi] = accv + Real(p.coef.wacc) * k;
+        if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
+      }
+      __syncthreads();
+    }
+  }
+  if (!ok && tid == 0)
+    for (int s = 0; s < C::NSLOT; ++s)
+      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 1000000000ull);
+}
+
+}  // namespace fvm

@@ -1,0 +1,566 @@
+// Fused Navier-Stokes stage kernel: residual (navier_stokes.py:588-711) and
+// the Runge-Kutta stage combination (time_integrators.py) in one pass.
+//
+// Tiling: a block owns a 32 x TY column tile of interior cells and marches a
+// chunk of ZC planes along x3.  Each step K (ghosted plane index):
+//   A  TMA brings plane K+HH of all 5 conserved variables (tile + HH halo)
+//      into a shared-memory ring (one mbarrier per slot, bounded waits);
+//   B  v = m/rho on plane K+3                         (viscous only)
+//   C  P on plane K+2                     (navier_stokes.py:94-100)
+//   D  Stokes stress on plane K+2, zero on ghosts     (viscous only, :102-142)
+//   E  x3 MUSCL slopes of cell K+1 for the block's columns (registers)
+//   F  x3 face flux at K+1/2 (registers; K-1/2 kept from the previous step)
+//   G  x1 and x2 slopes -> face states -> fluxes through shared memory,
+//      divergence, sources, stage combination, coalesced store of plane K.
+// HH = 3 with viscosity (tau at K+2 needs v at K+3), 2 without.
+#pragma once
+#include "fvm_common.cuh"
+
+namespace fvm {
+
+template <typename Real>
+struct NsParams {
+  Layout lay;
+  Metric<Real> met;
+  const Real* u0;     // step base state (ghosted layout), read at the cell
+  Real* out;          // stage output (interior written)
+  Real* acc;          // k accumulator (interior), may be null
+  const double* dt;   // device time step
+  const int* active;  // device flag: 0 once t > t_end (the step is a no-op)
+  StageCoef coef;
+  double gamma, mu, g1, g2, g3;
+  unsigned* status;
+  int zchunk, ntx, nty, nzc;
+};
+
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+constexpr int round_up(int a, int b) { return (a + b - 1) / b * b; }
+__device__ __forceinline__ int pmod(int a, int m) { int r = a % m; return r < 0 ? r + m : r; }
+
+template <typename Real, bool VISC, int TY>
+struct NsCfg {
+  static constexpr int TX = 32;
+  static constexpr int NT = TX * (TY + 2);
+  static constexpr int NV = 5;
+  static constexpr int HH = VISC ? 3 : 2;
+  static constexpr int W = 40;  // U/v ring column c <-> tile x offset c-4
+  static constexpr int ROWS = TY + 2 * HH;
+  static constexpr int PL = ROWS * W;  // one U/v field plane
+  static constexpr int NSLOT = HH + 2;
+  static constexpr int SLOT = round_up(NV * PL * (int)sizeof(Real), 128) / (int)sizeof(Real);
+  // P and tau planes cover the tile plus 2 cells: column c2 <-> x offset c2-2,
+  // row r2 <-> y offset r2-2
+  static constexpr int W2 = TX + 4;
+  static constexpr int R2 = TY + 4;
+  static constexpr int PL2 = W2 * R2;
+  static constexpr int NREC = VISC ? 9 : 6;
+  static constexpr int XB = cmax(TY * (TX + 2), (TY + 2) * TX);  // slopes of one field
+  static constexpr int FB = cmax(TY * (TX + 1), (TY + 1) * TX);  // fluxes of one variable
+  static constexpr int OFF_U = 0;
+  static constexpr int OFF_V = OFF_U + NSLOT * SLOT;
+  static constexpr int OFF_P = OFF_V + (VISC ? 3 * 3 * PL : 0);
+  static constexpr int OFF_T = OFF_P + 3 * PL2;
+  static constexpr int OFF_S = OFF_T + (VISC ? 3 * 6 * PL2 : 0);
+  static constexpr int OFF_FB = OFF_S + NREC * XB;
+  static constexpr int END = OFF_FB + 5 * FB;
+  static constexpr int BYTES = round_up(END * (int)sizeof(Real), 16) + NSLOT * 8;
+  static constexpr unsigned TX_BYTES = NV * PL * sizeof(Real);
+};
+
+// Normal fluxes and wave data of one face state along axis D
+// (navier_stokes.py:159-316).  q = [rho, m1, m2, m3, e, P, tau_D1, tau_D2, tau_D3].
+template <typename R, int D, bool VISC>
+__device__ __forceinline__ void ns_face(const R* q, R gam, R Fc[5], R Fd[5], R& vn, R& cs) {
+  const R rho = q[0];
+  R v0, v1, v2, E, ir = R(0);
+  if constexpr (sizeof(R) == 4) {
+    ir = rcp_approx(rho);
+    v0 = q[1] * ir; v1 = q[2] * ir; v2 = q[3] * ir; E = q[4] * ir;
+  } else {
+    v0 = q[1] / rho; v1 = q[2] / rho; v2 = q[3] / rho; E = q[4] / rho;
+  }
+  const R P = q[5];
+  const R va = D == 0 ? v0 : (D == 1 ? v1 : v2);
+  Fc[0] = rho * va;
+  Fc[1] = (rho * v0) * va;
+  Fc[2] = (rho * v1) * va;
+  Fc[3] = (rho * v2) * va;
+  Fc[1 + D] = Fc[1 + D] + P;
+  Fc[4] = ((rho * E) + P) * va;
+  if constexpr (VISC) {
+    Fd[0] = R(0);
+    Fd[1] = -q[6];
+    Fd[2] = -q[7];
+    Fd[3] = -q[8];
+    Fd[4] = (((-q[6]) * v0) - (q[7] * v1)) - (q[8] * v2);
+  }
+  if constexpr (sizeof(R) == 4) cs = sqrt_approx((gam * P) * ir);
+  else cs = sqrt((gam * P) / rho);
+  vn = va;
+}
+
+// Riemann flux + centred diffusive flux (riemann_solvers.py, diffusive_solvers.py).
+template <typename R, int D, int RIEM, bool VISC>
+__device__ __forceinline__ void ns_flux(const R* qL, const R* qR, R gam, R F[5]) {
+  R FcL[5], FcR[5], FdL[5], FdR[5], vnL, vnR, csL, csR;
+  ns_face<R, D, VISC>(qL, gam, FcL, FdL, vnL, csL);
+  ns_face<R, D, VISC>(qR, gam, FcR, FdR, vnR, csR);
+  if constexpr (RIEM == RIEM_HLL) {
+    const R smin = fmin(vnL - csL, vnR - csR);
+    const R smax = fmax(vnL + csL, vnR + csR);
+    const R den = smax - smin;
+    const R rden = recip(den);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const R num = ((smax * FcL[v]) - (smin * FcR[v])) + ((smin * smax) * (qR[v] - qL[v]));
+      R mid;
+      if constexpr (sizeof(R) == 4) mid = num * rden;
+      else mid = num / den;
+      F[v] = smin >= R(0) ? FcL[v] : (smax <= R(0) ? FcR[v] : mid);
+    }
+  } else {
+    const R vs = fmax(fabs(vnL) + csL, fabs(vnR) + csR);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F[v] = ((FcL[v] + FcR[v]) / R(2)) - ((vs * (qR[v] - qL[v])) / R(2));
+  }
+  if constexpr (VISC) {
+#pragma unroll
+    for (int v = 1; v < 5; ++v) F[v] = F[v] + ((FdL[v] + FdR[v]) / R(2));
+  }
+}
+
+template <typename Real, int LIM, int RIEM, int COORD, bool VISC, int TY, int MINB>
+__global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
+    ns_stage_kernel(const __grid_constant__ CUtensorMap tmap, const NsParams<Real> p) {
+  using C = NsCfg<Real, VISC, TY>;
+  using G = Geo<Real, COORD>;
+  constexpr int TX = C::TX, NT = C::NT, W = C::W, PL = C::PL, HH = C::HH, NREC = C::NREC;
+  constexpr int W2 = C::W2, PL2 = C::PL2;
+  constexpr bool F32 = sizeof(Real) == 4;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Real* sm = reinterpret_cast<Real*>(smem_raw);
+  Real* uring = sm + C::OFF_U;
+  Real* vring = sm + C::OFF_V;
+  Real* pring = sm + C::OFF_P;
+  Real* tring = sm + C::OFF_T;
+  Real* sl = sm + C::OFF_S;
+  Real* fb = sm + C::OFF_FB;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (C::BYTES - C::NSLOT * 8));
+
+  if (p.active && !*p.active) return;
+  if (smem_u32(smem_raw) & 127u) {  // TMA destinations need 128-byte alignment
+    if (threadIdx.x == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+    return;
+  }
+  const int tid = threadIdx.x;
+  const Layout& L = p.lay;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const Real gam = Real(p.gamma), mu = Real(p.mu);
+  const Real dt = Real(*p.dt);
+
+  if (tid == 0) {
+    tma_prefetch_desc(&tmap);
+    for (int s = 0; s < C::NSLOT; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  unsigned phase_bits = 0;  // expected parity per slot (identical in all threads)
+  unsigned pending = 0;     // slots with a load in flight (meaningful in thread 0)
+
+  // ring accessors: U/v in tile+HH coordinates (r, c), P/tau in tile+2 (r2, c2)
+  auto U = [&](int slot, int q, int r, int c) -> Real& { return uring[slot * C::SLOT + q * PL + r * W + c]; };
+  auto Vv = [&](int pl, int q, int r, int c) -> Real& { return vring[(pmod(pl, 3) * 3 + q) * PL + r * W + c]; };
+  auto Pp = [&](int pl, int r2, int c2) -> Real& { return pring[pmod(pl, 3) * PL2 + r2 * W2 + c2]; };
+  auto Tt = [&](int pl, int q, int r2, int c2) -> Real& {
+    return tring[(pmod(pl, 3) * 6 + q) * PL2 + r2 * W2 + c2];
+  };
+  // value of recon field f (U 0..4, P 5, tau row-d component 6..8) of plane K
+  // at tile offset (tx, ty); ti = tau indices of the row of the face axis
+  auto field = [&](int sK, int K, const int* ti, int f, int tx, int ty) -> Real {
+    if (f < 5) return U(sK, f, ty + HH, tx + 4);
+    if (f == 5) return Pp(K, ty + 2, tx + 2);
+    return Tt(K, ti[f - 6], ty + 2, tx + 2);
+  };
+
+  const bool is_out = tid < TX * TY;
+  const int otx = tid % TX, oty = tid / TX;
+
+  const int ntiles = p.ntx * p.nty * p.nzc;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int tx_i = tile % p.ntx;
+    const int ty_i = (tile / p.ntx) % p.nty;
+    const int zc_i = tile / (p.ntx * p.nty);
+    const int x0 = tx_i * TX, y0 = ty_i * TY;
+    const int Z0 = 1 + zc_i * p.zchunk;         // first ghosted output plane
+    const int Zl = min(Z0 + p.zchunk - 1, nz);  // last ghosted output plane
+    const int Pfirst = Z0 - HH, Plast = Zl + HH;
+    const int Kfirst = Z0 - 4;  // first step: P (and tau) of plane Z0-2
+
+    const int oi = x0 + otx, oj = y0 + oty;  // output cell (interior 0-based)
+    const bool out_valid = is_out && oi < nx && oj < ny;
+    Real zs[NREC];
+    Real Fzp[5], Fzn[5];
+#pragma unroll
+    for (int f = 0; f < NREC; ++f) zs[f] = Real(0);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) { Fzp[v] = Real(0); Fzn[v] = Real(0); }
+    const Real S3c = out_valid ? G::S3(p.met, oi, oj) : Real(0);
+
+    auto issue = [&](int pl) {
+      const int s = pmod(pl, C::NSLOT);
+      pending |= 1u << s;
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&bars[s], C::TX_BYTES);
+      tma_load_4d(&uring[s * C::SLOT], &tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
+    };
+    // planes needed by the first step plus one of prefetch
+    if (tid == 0)
+      for (int pl = Pfirst; pl <= Kfirst + HH + 1 && pl <= Plast; ++pl) issue(pl);
+
+    for (int K = Kfirst; K <= Zl; ++K) {
+      // ---------------------------------------------------------- A ----
+      if (tid == 0 && K > Kfirst && K + HH + 1 <= Plast) issue(K + HH + 1);
+      {
+        bool got = true;
+        for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= K + HH; ++pl) {
+          const int s = pmod(pl, C::NSLOT);
+          got = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 2000000000ull);
+          phase_bits ^= (1u << s);
+        }
+        if (!__syncthreads_and(got)) {
+          if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+          ok = false;
+          break;
+        }
+        if (tid == 0)
+          for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= K + HH; ++pl) pending &= ~(1u << pmod(pl, C::NSLOT));
+      }
+      const int sK = pmod(K, C::NSLOT), sK1 = pmod(K + 1, C::NSLOT), sK2 = pmod(K + 2, C::NSLOT);
+      // ---------------------------------------------------------- B ----
+      // v on the newest plane(s), tile + 3 (viscous only)
+      if constexpr (VISC) {
+        for (int pl = (K == Kfirst ? Pfirst : K + 3); pl <= K + 3; ++pl) {
+          const int s = pmod(pl, C::NSLOT);
+          for (int it = tid; it < C::ROWS * (TX + 6); it += NT) {
+            const int r = it / (TX + 6), c = 1 + it % (TX + 6);
+            const Real rho = U(s, 0, r, c);
+            if constexpr (F32) {
+              const Real ir = rcp_approx(rho);
+              Vv(pl, 0, r, c) = U(s, 1, r, c) * ir;
+              Vv(pl, 1, r, c) = U(s, 2, r, c) * ir;
+              Vv(pl, 2, r, c) = U(s, 3, r, c) * ir;
+            } else {
+              Vv(pl, 0, r, c) = U(s, 1, r, c) / rho;
+              Vv(pl, 1, r, c) = U(s, 2, r, c) / rho;
+              Vv(pl, 2, r, c) = U(s, 3, r, c) / rho;
+            }
+          }
+        }
+      }
+      // ---------------------------------------------------------- C ----
+      // P on plane K+2, tile + 2 (navier_stokes.py:94-100)
+      {
+        const int pl = K + 2;
+        for (int it = tid; it < C::PL2; it += NT) {
+          const int r2 = it / W2, c2 = it % W2;
+          const int r = r2 + HH - 2, c = c2 + 2;
+          const Real rho = U(sK2, 0, r, c);
+          Real v0, v1, v2, E;
+          if constexpr (F32) {
+            const Real ir = rcp_approx(rho);
+            v0 = U(sK2, 1, r, c) * ir; v1 = U(sK2, 2, r, c) * ir; v2 = U(sK2, 3, r, c) * ir;
+            E = U(sK2, 4, r, c) * ir;
+          } else {
+            v0 = U(sK2, 1, r, c) / rho; v1 = U(sK2, 2, r, c) / rho; v2 = U(sK2, 3, r, c) / rho;
+            E = U(sK2, 4, r, c) / rho;
+          }
+          Pp(pl, r2, c2) = ((gam - Real(1)) * rho) * (E - (((v0 * v0) + (v1 * v1)) + (v2 * v2)) / Real(2));
+        }
+      }
+      if constexpr (VISC) __syncthreads();
+      // ---------------------------------------------------------- D ----
+      // Stokes stress on plane K+2, tile + 2, zero on ghosts (:102-142)
+      if constexpr (VISC) {
+        const int pl = K + 2;
+        const int k = pl - 1;  // interior plane index
+        const bool zghost = (k < 0 || k >= nz);
+        for (int it = tid; it < C::PL2; it += NT) {
+          const int r2 = it / W2, c2 = it % W2;
+          const int r = r2 + 1, c = c2 + 2;
+          const int i = x0 + c2 - 2, j = y0 + r2 - 2;
+          Real t[6];
+          if (zghost || i < 0 || i >= nx || j < 0 || j >= ny) {
+#pragma unroll
+            for (int m = 0; m < 6; ++m) t[m] = Real(0);
+          } else {
+            Real g[3][3];  // g[cc][a] = d v_cc / d x_a
+            if constexpr (F32) {
+              const Real h1 = 0.5f * inv_len<Real, COORD, 0>(p.met, i, j, k);
+              const Real h2 = 0.5f * inv_len<Real, COORD, 1>(p.met, i, j, k);
+              const Real h3 = 0.5f * inv_len<Real, COORD, 2>(p.met, i, j, k);
+#pragma unroll
+              for (int cc = 0; cc < 3; ++cc) {
+                g[cc][0] = (Vv(pl, cc, r, c + 1) - Vv(pl, cc, r, c - 1)) * h1;
+                g[cc][1] = (Vv(pl, cc, r + 1, c) - Vv(pl, cc, r - 1, c)) * h2;
+                g[cc][2] = (Vv(pl + 1, cc, r, c) - Vv(pl - 1, cc, r, c)) * h3;
+              }
+            } else {
+              const Real l1 = G::L1(p.met, i, j, k), l2 = G::L2(p.met, i, j, k), l3 = G::L3(p.met, i, j, k);
+#pragma unroll
+              for (int cc = 0; cc < 3; ++cc) {
+                g[cc][0] = (Vv(pl, cc, r, c + 1) - Vv(pl, cc, r, c - 1)) / (Real(2) * l1);
+                g[cc][1] = (Vv(pl, cc, r + 1, c) - Vv(pl, cc, r - 1, c)) / (Real(2) * l2);
+                g[cc][2] = (Vv(pl + 1, cc, r, c) - Vv(pl - 1, cc, r, c)) / (Real(2) * l3);
+              }
+            }
+            const Real tt = Real(2.0 / 3.0);
+            if constexpr (COORD == COORD_CART) {
+              const Real divv = (g[0][0] + g[1][1]) + g[2][2];
+              t[0] = mu * ((Real(2) * g[0][0]) - (tt * divv));
+              t[1] = mu * ((Real(2) * g[1][1]) - (tt * divv));
+              t[2] = mu * ((Real(2) * g[2][2]) - (tt * divv));
+              t[3] = mu * (g[0][1] + g[1][0]);
+              t[4] = mu * (g[0][2] + g[2][0]);
+              t[5] = mu * (g[1][2] + g[2][1]);
+            } else {
+              Lame<Real> lm;
+              lame_at<Real, COORD>(p.met, i, j, lm);
+              const Real v0 = Vv(pl, 0, r, c), v1 = Vv(pl, 1, r, c), v2 = Vv(pl, 2, r, c);
+              const Real divv = (((((g[0][0] + g[1][1]) + g[2][2]) + ((v0 * (lm.dl[0][1] + lm.dl[0][2])) / lm.h[0])) +
+                                  ((v1 * (lm.dl[1][0] + lm.dl[1][2])) / lm.h[1])) +
+                                 ((v2 * (lm.dl[2][0] + lm.dl[2][1])) / lm.h[2]));
+              t[0] = mu * ((Real(2) * g[0][0]) - (tt * divv));
+              t[1] = mu * ((Real(2) * (g[1][1] + ((v0 * lm.dl[0][1]) / lm.h[0]))) - (tt * divv));
+              t[2] = mu * ((Real(2) * ((g[2][2] + ((v0 * lm.dl[0][2]) / lm.h[0])) + ((v1 * lm.dl[1][2]) / lm.h[1]))) -
+                           (tt * divv));
+              t[3] = mu * (((g[0][1] + g[1][0]) - ((v1 * lm.dl[0][1]) / lm.h[0])) + ((v0 * lm.dl[1][0]) / lm.h[1]));
+              t[4] = mu * (((g[0][2] + g[2][0]) - ((v2 * lm.dl[0][2]) / lm.h[0])) + ((v0 * lm.dl[2][0]) / lm.h[2]));
+              t[5] = mu * (((g[1][2] + g[2][1]) - ((v2 * lm.dl[1][2]) / lm.h[1])) + ((v1 * lm.dl[2][1]) / lm.h[2]));
+            }
+          }
+#pragma unroll
+          for (int m = 0; m < 6; ++m) Tt(pl, m, r2, c2) = t[m];
+        }
+      }
+      __syncthreads();
+      // -------------------------------------------------------- E, F ----
+      // x3 slopes of cell K+1 and the x3 face flux at K+1/2 (registers);
+      // tau row 3 = (t13, t23, t33)
+      if (K >= Z0 - 2 && is_out) {
+        constexpr int ti[3] = {4, 5, 2};
+        const int kk = K;  // interior index of plane K+1
+        const bool ghost = (K + 1 <= 0 || K + 1 >= nz + 1);
+        Real zn[NREC];
+        Real qm[NREC], q0[NREC], qp[NREC];
+#pragma unroll
+        for (int f = 0; f < NREC; ++f) {
+          qm[f] = field(sK, K, ti, f, otx, oty);
+          q0[f] = field(sK1, K + 1, ti, f, otx, oty);
+          qp[f] = field(sK2, K + 2, ti, f, otx, oty);
+        }
+        if (ghost || !out_valid) {
+#pragma unroll
+          for (int f = 0; f < NREC; ++f) zn[f] = Real(0);
+        } else {
+          const Real l3 = F32 ? Real(1) : G::L3(p.met, oi, oj, kk);
+#pragma unroll
+          for (int f = 0; f < NREC; ++f) zn[f] = muscl_slope<LIM>(qm[f], q0[f], qp[f], l3);
+        }
+        if (K >= Z0 - 1) {
+          Real qL[NREC], qR[NREC], F[5];
+#pragma unroll
+          for (int f = 0; f < NREC; ++f) {
+            qL[f] = qm[f] + zs[f] / Real(2);
+            qR[f] = q0[f] - zn[f] / Real(2);
+          }
+          ns_flux<Real, 2, RIEM, VISC>(qL, qR, gam, F);
+#pragma unroll
+          for (int v = 0; v < 5; ++v) { Fzp[v] = Fzn[v]; Fzn[v] = F[v] * S3c; }
+        }
+#pragma unroll
+        for (int f = 0; f < NREC; ++f) zs[f] = zn[f];
+      }
+      if (K < Z0) { __syncthreads(); continue; }
+      const int kK = K - 1;  // interior index of the output plane
+      // ------------------------------------------------ G: x1 slopes ----
+      {
+        constexpr int ti[3] = {0, 3, 4};  // tau row 1 = (t11, t12, t13)
+        for (int it = tid; it < TY * (TX + 2); it += NT) {
+          const int ty = it / (TX + 2), tx = it % (TX + 2) - 1;
+          const int i = x0 + tx, j = y0 + ty;
+          const bool interior = i >= 0 && i < nx && j < ny;
+          const Real l1 = (F32 || !interior) ? Real(1) : G::L1(p.met, i, j, kK);
+#pragma unroll
+          for (int f = 0; f < NREC; ++f) {
+            const Real s = interior ? muscl_slope<LIM>(field(sK, K, ti, f, tx - 1, ty), field(sK, K, ti, f, tx, ty),
+                                                       field(sK, K, ti, f, tx + 1, ty), l1)
+                                    : Real(0);
+            sl[f * C::XB + it] = s;
+          }
+        }
+      }
+      __syncthreads();
+      {
+        constexpr int ti[3] = {0, 3, 4};
+        for (int it = tid; it < TY * (TX + 1); it += NT) {
+          const int ty = it / (TX + 1), fx = it % (TX + 1);
+          const int fi = x0 + fx, j = y0 + ty;
+          Real F[5] = {Real(0), Real(0), Real(0), Real(0), Real(0)};
+          if (fi <= nx && j < ny) {
+            Real qL[NREC], qR[NREC];
+            const int oL = ty * (TX + 2) + fx;  // slope slot of the left cell (tx = fx-1)
+#pragma unroll
+            for (int f = 0; f < NREC; ++f) {
+              qL[f] = field(sK, K, ti, f, fx - 1, ty) + sl[f * C::XB + oL] / Real(2);
+              qR[f] = field(sK, K, ti, f, fx, ty) - sl[f * C::XB + oL + 1] / Real(2);
+            }
+            ns_flux<Real, 0, RIEM, VISC>(qL, qR, gam, F);
+            const Real s1 = G::S1(p.met, fi, j, kK);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) F[v] = F[v] * s1;
+          }
+#pragma unroll
+          for (int v = 0; v < 5; ++v) fb[v * C::FB + it] = F[v];
+        }
+      }
+      __syncthreads();
+      Real Fxm[5], Fxp[5];
+      if (is_out) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          Fxm[v] = fb[v * C::FB + oty * (TX + 1) + otx];
+          Fxp[v] = fb[v * C::FB + oty * (TX + 1) + otx + 1];
+        }
+      }
+      // ------------------------------------------------ G: x2 slopes ----
+      {
+        constexpr int ti[3] = {3, 1, 5};  // tau row 2 = (t12, t22, t23)
+        for (int it = tid; it < (TY + 2) * TX; it += NT) {
+          const int ty = it / TX - 1, tx = it % TX;
+          const int i = x0 + tx, j = y0 + ty;
+          const bool interior = i < nx && j >= 0 && j < ny;
+          const Real l2 = (F32 || !interior) ? Real(1) : G::L2(p.met, i, j, kK);
+#pragma unroll
+          for (int f = 0; f < NREC; ++f) {
+            const Real s = interior ? muscl_slope<LIM>(field(sK, K, ti, f, tx, ty - 1), field(sK, K, ti, f, tx, ty),
+                                                       field(sK, K, ti, f, tx, ty + 1), l2)
+                                    : Real(0);
+            sl[f * C::XB + it] = s;
+          }
+        }
+      }
+      __syncthreads();
+      {
+        constexpr int ti[3] = {3, 1, 5};
+        for (int it = tid; it < (TY + 1) * TX; it += NT) {
+          const int fy = it / TX, tx = it % TX;
+          const int fj = y0 + fy, i = x0 + tx;
+          Real F[5] = {Real(0), Real(0), Real(0), Real(0), Real(0)};
+          if (fj <= ny && i < nx) {
+            Real qL[NREC], qR[NREC];
+            const int oL = fy * TX + tx;  // slope slot of the lower cell (ty = fy-1)
+#pragma unroll
+            for (int f = 0; f < NREC; ++f) {
+              qL[f] = field(sK, K, ti, f, tx, fy - 1) + sl[f * C::XB + oL] / Real(2);
+              qR[f] = field(sK, K, ti, f, tx, fy) - sl[f * C::XB + oL + TX] / Real(2);
+            }
+            ns_flux<Real, 1, RIEM, VISC>(qL, qR, gam, F);
+            const Real s2 = G::S2(p.met, i, fj, kK);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) F[v] = F[v] * s2;
+          }
+#pragma unroll
+          for (int v = 0; v < 5; ++v) fb[v * C::FB + it] = F[v];
+        }
+      }
+      __syncthreads();
+      // ------------------------------------------------- G: output ----
+      if (out_valid) {
+        const int r = oty + HH, c = otx + 4;
+        Real q[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) q[v] = U(sK, v, r, c);
+        const Real rho = q[0];
+        Real v0, v1, v2;
+        if constexpr (F32) {
+          const Real ir = rcp_approx(rho);
+          v0 = q[1] * ir; v1 = q[2] * ir; v2 = q[3] * ir;
+        } else {
+          v0 = q[1] / rho; v1 = q[2] / rho; v2 = q[3] / rho;
+        }
+        // sources: geometric (navier_stokes.py:437-452) + gravity (:499-504)
+        Real src[5];
+        const Real gx = Real(p.g1), gy = Real(p.g2), gz = Real(p.g3);
+        src[0] = Real(0);
+        src[1] = rho * gx;
+        src[2] = rho * gy;
+        src[3] = rho * gz;
+        src[4] = rho * (((gx * v0) + (gy * v1)) + (gz * v2));
+        if constexpr (COORD != COORD_CART) {
+          Lame<Real> lm;
+          lame_at<Real, COORD>(p.met, oi, oj, lm);
+          const Real P = Pp(K, oty + 2, otx + 2);
+          const Real vv[3] = {v0, v1, v2};
+          Real tc[3][3];
+          if constexpr (VISC) {
+            const int r2 = oty + 2, c2 = otx + 2;
+            tc[0][0] = Tt(K, 0, r2, c2); tc[1][1] = Tt(K, 1, r2, c2); tc[2][2] = Tt(K, 2, r2, c2);
+            tc[0][1] = tc[1][0] = Tt(K, 3, r2, c2);
+            tc[0][2] = tc[2][0] = Tt(K, 4, r2, c2);
+            tc[1][2] = tc[2][1] = Tt(K, 5, r2, c2);
+          } else {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+              for (int b = 0; b < 3; ++b) tc[a][b] = Real(0);
+          }
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc) {
+            const int o0 = cc == 0 ? 1 : 0, o1 = cc == 2 ? 1 : 2;
+            const Real sgc = (((((P * lm.d123[cc]) / lm.h[cc]) + ((((rho * vv[o0]) * vv[o0]) * lm.dl[cc][o0]) / lm.h[cc])) +
+                               ((((rho * vv[o1]) * vv[o1]) * lm.dl[cc][o1]) / lm.h[cc])) -
+                              ((((rho * vv[cc]) * vv[o0]) * lm.dl[o0][cc]) / lm.h[o0])) -
+                             ((((rho * vv[cc]) * vv[o1]) * lm.dl[o1][cc]) / lm.h[o1]);
+            const Real sgd = ((((tc[cc][o0] * lm.dl[o0][cc]) / lm.h[o0]) + ((tc[cc][o1] * lm.dl[o1][cc]) / lm.h[o1])) -
+                              ((tc[o0][o0] * lm.dl[cc][o0]) / lm.h[cc])) -
+                             ((tc[o1][o1] * lm.dl[cc][o1]) / lm.h[cc]);
+            src[1 + cc] = (sgc + sgd) + src[1 + cc];
+          }
+        }
+        const Real Vc = G::V(p.met, oi, oj, kK);
+        const Real iV = recip(Vc);
+        const long long gidx = L.idx(0, K, oj + 1, oi + 1);
+        unsigned bad = 0;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const Real Fym = fb[v * C::FB + oty * TX + otx];
+          const Real Fyp = fb[v * C::FB + (oty + 1) * TX + otx];
+          const Real sum = ((((Fxp[v] - Fxm[v]) + Fyp) - Fym) + Fzn[v]) - Fzp[v];
+          Real k;
+          if constexpr (F32) k = (-sum) * iV + src[v];
+          else k = (-sum) / Vc + src[v];
+          const long long gi = gidx + (long long)v * L.var_stride;
+          Real u0v = Real(0), accv = Real(0);
+          if (p.coef.mode >= MODE_AXPY) u0v = p.u0[gi];
+          if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
+          const Real o = stage_combine(p.coef, dt, k, q[v], u0v, accv);
+          p.out[gi] = o;
+          if (p.coef.accmode == ACC_SET) p.acc[gi] = k;
+          else if (p.coef.accmode == ACC_ADD) p.acc[gi] = accv + Real(p.coef.wacc) * k;
+          if (!isfinite(o)) bad |= ST_NONFINITE;
+          if (v == 0 && p.coef.mode != MODE_RHS && !(o > Real(0))) bad |= ST_DENSITY;
+        }
+        if (bad) atomicOr(p.status, bad);
+      }
+      __syncthreads();
+    }
+  }
+  // On a timeout, wait (bounded) for every load this block may still have in flight.
+  if (!ok && tid == 0) {
+    for (int s = 0; s < C::NSLOT; ++s)
+      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 1000000000ull);
+  }
+}
+
+}  // namespace fvm

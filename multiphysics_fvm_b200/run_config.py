@@ -1,0 +1,63 @@
+"""Run a benchmark configuration for a few steps (used for profiling).
+
+    python -m multiphysics_fvm_b200.run_config rt3d --n 256 --steps 2 [--precision fp32]
+    python -m multiphysics_fvm_b200.run_config kh2d --n 256 --steps 200
+
+Configurations: kh2d (2D sharp Kelvin-Helmholtz), kh3d (its 3D extrusion),
+rt3d (3D Rayleigh-Taylor), maxwell_sph (spherical pulse), heat_cyl
+(cylindrical hot spot).  Prints the device time per step.
+"""
+from __future__ import annotations
+
+import argparse
+import math
+
+import numpy as np
+
+from . import backend
+from .grid.geometry import build_grid
+
+
+def make(name: str, n: int, precision: str | None = None):
+    from .setups import kelvin_helmholtz_sharp as kh, rayleigh_taylor_3d as rt
+    if name == "kh2d":
+        s = kh.get_setup(n, n, 1)
+    elif name == "kh3d":
+        s = kh.get_setup(n, n, n, precision="fp32")
+    elif name == "rt3d":
+        s = rt.get_setup(n, n, n)
+    elif name == "maxwell_sph":
+        from .setups import maxwell_spherical_pulse as mx
+        s = mx.get_setup(n // 2, n // 2, n)
+    elif name == "heat_cyl":
+        from .setups import heat_cylindrical_hotspot as hc
+        s = hc.get_setup(3 * n // 4, n, n // 2)
+    else:
+        raise ValueError(f"unknown configuration {name!r}")
+    if precision:
+        s["precision"] = precision
+    g = build_grid(s["coordinate_system"], s["grid_config"])
+    U = s["physics"].allocate_u(s["grid_config"])
+    s["initial_conditions"]["initializer"](U, s["physical_parameters"], g, s["initial_conditions"]["parameters"])
+    return s, np.stack([U[k] for k in backend.VARIABLES[backend.physics_name(s["physics"])]])
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("config")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--precision", default=None)
+    a = ap.parse_args()
+    s, U = make(a.config, a.n, a.precision)
+    sim = backend.Simulation.from_setup(s)
+    sim.upload(U)
+    sim.set_time(0.0, math.inf, float(s["time_config"]["CFL"]))
+    sim.step(a.warmup)
+    ms = sim.time_steps(a.steps)
+    print(f"{a.config} n={a.n} {s.get('precision')}: {ms / a.steps:.3f} ms/step, status={sim.status()}")
+
+
+if __name__ == "__main__":
+    main()
