@@ -43,6 +43,22 @@ STAGE_BYTES = [60.0, 100.0, 60.0]
 DT_BYTES = 20.0
 
 
+def reduce_max(dist, value, device="cuda"):
+    """Max over ranks of a per-rank duration (identity without a process group)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, cells, steps, seconds):
+    """Whole-job cell-updates/s of `world` replicas that each advanced `cells`
+    cells `steps` times, with `seconds` the max over ranks."""
+    return world * cells * steps / seconds
+
+
 def env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
@@ -144,7 +160,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     import multiprocessing as mp
-    cores = os.cpu_count() or 1
+    cores = min(os.cpu_count() or 1, 64)
     n = 32  # per-process sample: 32^3 cells of the same setup and schemes
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
@@ -190,12 +206,9 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         ms = sim.time_steps(args.steps)
     barrier()
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(dist, ms)
     status = sim.status()
-    value = world * cells * args.steps / (ms / 1e3)
+    value = aggregate_rate(world, cells, args.steps, ms / 1e3)
 
     # dominant kernel: per-launch device time of the stage kernels (events)
     stage_ms, other_ms, launches = sim.profile_steps(max(3, min(args.steps, 10)))
@@ -225,11 +238,8 @@ def run_ours(args):
         sim.download(out)
     barrier()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * cells * e2e_steps / e2e_s
+    e2e_s = reduce_max(dist, e2e_s)
+    e2e = aggregate_rate(world, cells, e2e_steps, e2e_s)
 
     if rank == 0:
         cpu_v, cpu_el = cpu_baseline_sample()
