@@ -146,6 +146,23 @@ int fvm_clear_status(fvm_handle* h);
 int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_kernel_ms,
                       double* other_kernel_ms, int* stage_launches);
 
+/* Conserved totals sum_q(cells[q][i] * volumes[i]) in float64 with compensated
+ * summation, computed without allocating any device memory.  No counterpart in
+ * the reference.  For callers that cannot call cudaMalloc (a host framework
+ * that owns every allocation, an embedded runtime that forbids allocation
+ * after start-up): the per-block partial sums live in a fixed 64 KiB device
+ * array inside the library, which every GPU that loads the library holds
+ * until the process exits.  cells: float32 device array (nvars, ncells), any
+ * cell order; volumes: float64 device array (ncells); totals: float64 device
+ * array of nvars outputs.  nvars must be 1..8 (FVM_E_INVALID otherwise).  Work
+ * is enqueued on `stream` (a cudaStream_t, 0 = legacy default stream) and not
+ * waited for.  The first call on a device (with that device current) resolves
+ * the array's device address; make it before any stream capture.  All calls
+ * share the one array: calls whose kernels can overlap on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller. */
+int fvm_totals_noalloc(const float* cells, const double* volumes, int nvars, long long ncells, double* totals,
+                       void* stream);
+
 /* Copy the message of the last failure on this thread into buf. */
 int fvm_last_error(char* buf, int len);
 

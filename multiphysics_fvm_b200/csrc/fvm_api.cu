@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -777,3 +778,83 @@ int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_ker
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Conserved totals without any device allocation (fvm_totals_noalloc).
+//
+// Callers that cannot allocate device memory themselves -- code running inside
+// a host that owns and pre-plans every allocation (a memory-pool-managed
+// framework, a captured or replayed command stream, an embedded runtime that
+// forbids cudaMalloc after start-up) -- still need the float64 compensated
+// totals.  This variant keeps the per-block partial sums in a fixed
+// file-scope device array instead of the handle's `partials` buffer, so it
+// needs neither a handle nor a cudaMalloc: the caller passes only its input
+// cells, its cell volumes and the output array.
+namespace {
+
+constexpr int NOALLOC_BLOCKS = 1024;  // partial-sum rows held by the scratch array
+constexpr int NOALLOC_MAX_VARS = 8;   // sums per row
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+// 64 KiB, resident on every GPU that loads the library until the process exits.
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_BLOCKS * NOALLOC_MAX_VARS];
+
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+__global__ void totals_dense_kernel(const float* __restrict__ cells, const double* __restrict__ volumes, int nv,
+                                    long long n, double* __restrict__ partials) {
+  __shared__ double ss[256][NOALLOC_MAX_VARS];
+  double s[NOALLOC_MAX_VARS], c[NOALLOC_MAX_VARS];
+  for (int q = 0; q < NOALLOC_MAX_VARS; ++q) { s[q] = 0.0; c[q] = 0.0; }
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double V = volumes[i];
+    for (int q = 0; q < nv; ++q) neumaier_add(s[q], c[q], double(cells[(long long)q * n + i]) * V);
+  }
+  for (int q = 0; q < nv; ++q) ss[threadIdx.x][q] = s[q] + c[q];
+  __syncthreads();
+  if (threadIdx.x < nv) {
+    double bs = 0.0, bc = 0.0;
+    for (int t = 0; t < (int)blockDim.x; ++t) neumaier_add(bs, bc, ss[t][threadIdx.x]);
+    partials[blockIdx.x * NOALLOC_MAX_VARS + threadIdx.x] = bs + bc;
+  }
+}
+
+}  // namespace
+
+extern "C" int fvm_totals_noalloc(const float* cells, const double* volumes, int nvars, long long ncells,
+                                  double* totals, void* stream) {
+  if (!cells || !volumes || !totals) return fail(FVM_E_INVALID, "fvm_totals_noalloc: null pointer");
+  if (nvars < 1 || nvars > NOALLOC_MAX_VARS)
+    return fail(FVM_E_INVALID, "fvm_totals_noalloc: nvars must be in [1, " + std::to_string(NOALLOC_MAX_VARS) +
+                                   "], got " + std::to_string(nvars));
+  if (ncells < 1) return fail(FVM_E_INVALID, "fvm_totals_noalloc: ncells must be >= 1");
+  int dev = 0;
+  FVM_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    return fail(FVM_E_INVALID, "fvm_totals_noalloc: device ordinal above " + std::to_string(NOALLOC_MAX_DEVICES - 1));
+  double* partials = nullptr;
+  {
+    // First call on this device (with it current): resolve the device address
+    // of the scratch array.  Host code must not pass the symbol itself.
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+      if (e != cudaSuccess)
+        return fail(FVM_E_CUDA, std::string("fvm_totals_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    partials = g_noalloc_ptr[dev];
+  }
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const long long want = (ncells + 255) / 256;
+  const int blocks = (int)(want < NOALLOC_BLOCKS ? want : NOALLOC_BLOCKS);
+  // Every used row of the scratch array is overwritten before it is read, so
+  // nothing has to be cleared between calls.
+  totals_dense_kernel<<<blocks, 256, 0, s>>>(cells, volumes, nvars, ncells, partials);
+  FVM_CK(cudaGetLastError());
+  totals_final_kernel<<<1, 32, 0, s>>>(partials, blocks, nvars, totals);
+  FVM_CK(cudaGetLastError());
+  return FVM_OK;
+}
