@@ -242,6 +242,7 @@ void fill_common(fvm_handle* h, const StageDef& sd, bool rhs_only, P& p) {
   p.coef.ca = sd.ca;
   p.coef.cb = sd.cb;
   p.coef.wacc = sd.w;
+  p.coef.u0_is_input = sd.in == 0 ? 1 : 0;
   p.status = h->status;
   p.zchunk = h->zchunk;
 }
@@ -254,6 +255,7 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
     HeatParams<Real> p{};
     fill_common<Real>(h, sd, rhs_only, p);
     p.rho_cp = d.params[0] * d.params[1];
+    p.inv_rho_cp = 1.0 / (d.params[0] * d.params[1]);
     p.k = d.params[2];
     p.q = d.params[3];
     return launch_heat<Real>(kernel_limiter(d), d.coords, h->tmap[sd.in], p, h->stream, nsm);
@@ -283,6 +285,7 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
   p.coef.ca = sd.ca;
   p.coef.cb = sd.cb;
   p.coef.wacc = sd.w;
+  p.coef.u0_is_input = sd.in == 0 ? 1 : 0;
   p.gamma = d.params[0];
   p.mu = d.params[1];
   p.g1 = d.params[2];
@@ -498,7 +501,7 @@ int fvm_create(const fvm_desc* desc, fvm_handle** out) {
   const bool visc = d.physics == FVM_NAVIER_STOKES && d.params[1] != 0.0;
   int rows;
   if (d.physics == FVM_HEAT) rows = 8 + (d.reconstructor == FVM_PIECEWISE_CONSTANT ? 4 : 6);
-  else if (d.physics == FVM_MAXWELL) rows = 8 + 4;
+  else if (d.physics == FVM_MAXWELL) rows = (h->f64 ? maxwell_tile_ty<double>() : maxwell_tile_ty<float>()) + 4;
   else if (h->f64) rows = visc ? ns_tile_ty<double, true>() + 6 : ns_tile_ty<double, false>() + 4;
   else rows = visc ? ns_tile_ty<float, true>() + 6 : ns_tile_ty<float, false>() + 4;
   for (int b = 0; b < 3; ++b) {

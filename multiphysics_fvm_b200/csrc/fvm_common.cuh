@@ -292,7 +292,14 @@ __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap* map) {
 struct StageCoef {
   int mode, accmode;
   double ca, cb, wacc;  // mode constants (see StageMode), acc weight
+  int u0_is_input;      // the stage input buffer is the step base U0 (first stage)
 };
+
+// Ask L2 for the 128-byte line holding p (the epilogue's U0/acc rows), so the
+// dependent loads at the end of a z-march step hit L2 instead of DRAM.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 
 // Combine one variable.  `k` is the residual, `ucur` the stage input, `u0`
 // the step's base state, `acc` the running k-sum.  Op order follows

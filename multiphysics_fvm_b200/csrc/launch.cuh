@@ -127,11 +127,15 @@ extern template cudaError_t launch_heat<float>(int, int, const CUtensorMap&, con
 extern template cudaError_t launch_heat<double>(int, int, const CUtensorMap&, const HeatParams<double>&, cudaStream_t, int);
 
 // ------------------------------------------------------------- maxwell ----
+// Maxwell: 6 rows x 32 columns, 2 blocks of 256 threads per SM (float32).
+template <typename Real>
+constexpr int maxwell_tile_ty() { return std::is_same<Real, double>::value ? 8 : 6; }
+
 template <typename Real, int LIM, int RIEM, int COORD>
 cudaError_t launch_maxwell_one(const CUtensorMap& map, MaxwellParams<Real> p, cudaStream_t s, int nsm) {
-  constexpr int TY = 8;
+  constexpr int TY = maxwell_tile_ty<Real>();
   using C = MaxwellCfg<Real, TY>;
-  auto kern = maxwell_stage_kernel<Real, LIM, RIEM, COORD, TY>;
+  auto kern = maxwell_stage_kernel<Real, LIM, RIEM, COORD, TY, std::is_same<Real, double>::value ? 1 : 2>;
   static int bps = 0;
   if (bps == 0 || nsm < 0) {
     cudaError_t e = prepare_kernel(kern, C::NT, C::BYTES, &bps);

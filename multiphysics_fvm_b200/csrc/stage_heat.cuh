@@ -23,7 +23,7 @@ struct HeatParams {
   const double* dt;
   const int* active;
   StageCoef coef;
-  double rho_cp, k, q;
+  double rho_cp, k, q, inv_rho_cp;
   unsigned* status;
   int zchunk, ntx, nty, nzc;
 };
@@ -74,7 +74,8 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
   const int tid = threadIdx.x;
   const Layout& L = p.lay;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
-  const Real rcp = Real(p.rho_cp), kk = Real(p.k), qsrc = Real(p.q);
+  const Real rcp = Real(p.rho_cp), kk = Real(p.k), qsrc = Real(p.q), ircp = Real(p.inv_rho_cp);
+  constexpr bool F32 = sizeof(Real) == 4;
   const Real dt = Real(*p.dt);
   if (tid == 0) {
     tma_prefetch_desc(&tmap);
@@ -124,9 +125,12 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
       // T on the newest plane (heat.py:74)
       {
         const int pl = K + HH;
+        const Real* ub = uring + pmod(pl, C::NSLOT) * C::SLOT;
+        Real* tb = tring + pmod(pl, 3) * PL;
         for (int it = tid; it < C::ROWS * (TX + 6); it += NT) {
-          const int r = it / (TX + 6), c = 1 + it % (TX + 6);
-          T(pl, r, c) = U(pl, r, c) / rcp;
+          const int o = (it / (TX + 6)) * W + 1 + it % (TX + 6);
+          if constexpr (F32) tb[o] = ub[o] * ircp;
+          else tb[o] = ub[o] / rcp;
         }
       }
       __syncthreads();
@@ -136,19 +140,32 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         constexpr int PH = HH - 1;
         const int pl = K + HH - 1, k = pl - 1;
         const bool zg = k < 0 || k >= nz;
+        const Real* tm = tring + pmod(pl - 1, 3) * PL;
+        const Real* t0 = tring + pmod(pl, 3) * PL;
+        const Real* tp = tring + pmod(pl + 1, 3) * PL;
+        Real* pw = phring + pmod(pl, 3) * 3 * PL;
         for (int it = tid; it < (TY + 2 * PH) * (TX + 2 * PH); it += NT) {
           const int r = HH - PH + it / (TX + 2 * PH), c = 4 - PH + it % (TX + 2 * PH);
           const int i = x0 + c - 4, j = y0 + r - HH;
           Real f0 = Real(0), f1 = Real(0), f2 = Real(0);
           if (!(zg || i < 0 || i >= nx || j < 0 || j >= ny)) {
-            const Real l1 = G::L1(p.met, i, j, k), l2 = G::L2(p.met, i, j, k), l3 = G::L3(p.met, i, j, k);
-            f0 = (-kk) * ((T(pl, r, c + 1) - T(pl, r, c - 1)) / (Real(2) * l1));
-            f1 = (-kk) * ((T(pl, r + 1, c) - T(pl, r - 1, c)) / (Real(2) * l2));
-            f2 = (-kk) * ((T(pl + 1, r, c) - T(pl - 1, r, c)) / (Real(2) * l3));
+            const int o = r * W + c;
+            if constexpr (F32) {
+              const Real h = -0.5f * kk;
+              f0 = (t0[o + 1] - t0[o - 1]) * (h * inv_len<Real, COORD, 0>(p.met, i, j, k));
+              f1 = (t0[o + W] - t0[o - W]) * (h * inv_len<Real, COORD, 1>(p.met, i, j, k));
+              f2 = (tp[o] - tm[o]) * (h * inv_len<Real, COORD, 2>(p.met, i, j, k));
+            } else {
+              const Real l1 = G::L1(p.met, i, j, k), l2 = G::L2(p.met, i, j, k), l3 = G::L3(p.met, i, j, k);
+              f0 = (-kk) * ((t0[o + 1] - t0[o - 1]) / (Real(2) * l1));
+              f1 = (-kk) * ((t0[o + W] - t0[o - W]) / (Real(2) * l2));
+              f2 = (-kk) * ((tp[o] - tm[o]) / (Real(2) * l3));
+            }
           }
-          Ph(pl, 0, r, c) = f0;
-          Ph(pl, 1, r, c) = f1;
-          Ph(pl, 2, r, c) = f2;
+          const int o = r * W + c;
+          pw[o] = f0;
+          pw[PL + o] = f1;
+          pw[2 * PL + o] = f2;
         }
       }
       __syncthreads();
@@ -171,6 +188,40 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
       }
       if (K < Z0) { __syncthreads(); continue; }
       const int kK = K - 1;
+      if constexpr (LIM == LIM_PC) {
+        // Piecewise-constant faces: phi_L, phi_R are the cell values, so each
+        // output cell forms its four in-plane face fluxes straight from the
+        // phi ring (no exchange phases).
+        if (out_valid) {
+          const Real* p0 = phring + pmod(K, 3) * 3 * PL + (oty + HH) * W + otx + 4;  // phi_1 at the cell
+          const Real* p1 = p0 + PL;                                                   // phi_2
+          const Real Fxm = (Real(0) + (p0[-1] + p0[0]) / Real(2)) * G::S1(p.met, oi, oj, kK);
+          const Real Fxp = (Real(0) + (p0[0] + p0[1]) / Real(2)) * G::S1(p.met, oi + 1, oj, kK);
+          const Real Fym = (Real(0) + (p1[-W] + p1[0]) / Real(2)) * G::S2(p.met, oi, oj, kK);
+          const Real Fyp = (Real(0) + (p1[0] + p1[W]) / Real(2)) * G::S2(p.met, oi, oj + 1, kK);
+          const Real sum = ((((Fxp - Fxm) + Fyp) - Fym) + Fzn) - Fzp;
+          Real k;
+          if constexpr (F32) k = (-sum) * rcp_approx(G::V(p.met, oi, oj, kK)) + qsrc;
+          else k = (-sum) / G::V(p.met, oi, oj, kK) + qsrc;
+          const long long gi = L.idx(0, K, oj + 1, oi + 1);
+          const Real ucur = U(K, oty + HH, otx + 4);
+          Real u0v = Real(0), accv = Real(0);
+          if (p.coef.mode >= MODE_AXPY) u0v = p.coef.u0_is_input ? ucur : p.u0[gi];
+          if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
+          const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
+          p.out[gi] = o;
+          if (p.coef.accmode == ACC_SET) p.acc[gi] = k;
+          else if (p.coef.accmode == ACC_ADD) p.acc[gi] = accv + Real(p.coef.wacc) * k;
+          if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
+        }
+        __syncthreads();
+        continue;
+      }
+      if (out_valid && otx == 0) {
+        const long long g0 = L.idx(0, K, oj + 1, oi + 1);
+        if (p.coef.mode >= MODE_AXPY && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0);
+        if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) prefetch_l2(p.acc + g0);
+      }
       // x1 faces of plane K
       for (int it = tid; it < TY * (TX + 2); it += NT) {
         const int ty = it / (TX + 2), tx = it % (TX + 2) - 1;
@@ -224,11 +275,13 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
       if (out_valid) {
         const Real Fym = fb[oty * TX + otx], Fyp = fb[(oty + 1) * TX + otx];
         const Real sum = ((((Fxp - Fxm) + Fyp) - Fym) + Fzn) - Fzp;
-        const Real k = (-sum) / G::V(p.met, oi, oj, kK) + qsrc;
+        Real k;
+        if constexpr (F32) k = (-sum) * rcp_approx(G::V(p.met, oi, oj, kK)) + qsrc;
+        else k = (-sum) / G::V(p.met, oi, oj, kK) + qsrc;
         const long long gi = L.idx(0, K, oj + 1, oi + 1);
         const Real ucur = U(K, oty + HH, otx + 4);
         Real u0v = Real(0), accv = Real(0);
-        if (p.coef.mode >= MODE_AXPY) u0v = p.u0[gi];
+        if (p.coef.mode >= MODE_AXPY) u0v = p.coef.u0_is_input ? ucur : p.u0[gi];
         if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
         const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
         p.out[gi] = o;

@@ -58,8 +58,15 @@ struct MaxwellCfg {
 // FD12 = -H3, FD13 = H2, FD23 = -H1 and antisymmetry (maxwell.py:145-165).
 template <typename R, int D>
 __device__ __forceinline__ void maxwell_face(const R* q, R mu, R ep, R F[6]) {
-  const R H0 = q[0] / mu, H1 = q[1] / mu, H2 = q[2] / mu;
-  const R E0 = q[3] / ep, E1 = q[4] / ep, E2 = q[5] / ep;
+  R H0, H1, H2, E0, E1, E2;
+  if constexpr (sizeof(R) == 4) {
+    const R imu = rcp_approx(mu), iep = rcp_approx(ep);
+    H0 = q[0] * imu; H1 = q[1] * imu; H2 = q[2] * imu;
+    E0 = q[3] * iep; E1 = q[4] * iep; E2 = q[5] * iep;
+  } else {
+    H0 = q[0] / mu; H1 = q[1] / mu; H2 = q[2] / mu;
+    E0 = q[3] / ep; E1 = q[4] / ep; E2 = q[5] / ep;
+  }
   if constexpr (D == 0) {
     F[0] = R(0); F[1] = -E2; F[2] = E1;
     F[3] = R(0); F[4] = H2; F[5] = -H1;
@@ -81,7 +88,9 @@ __device__ __forceinline__ void maxwell_flux(const R* qL, const R* qR, R mu, R e
   for (int v = 0; v < 6; ++v) {
     if constexpr (RIEM == RIEM_HLL) {
       const R smin = -c, smax = c;
-      F[v] = (((smax * FL[v]) - (smin * FR[v])) + ((smin * smax) * (qR[v] - qL[v]))) / (smax - smin);
+      const R num = ((smax * FL[v]) - (smin * FR[v])) + ((smin * smax) * (qR[v] - qL[v]));
+      if constexpr (sizeof(R) == 4) F[v] = num * (0.5f * rcp_approx(c));
+      else F[v] = num / (smax - smin);
     } else {
       F[v] = ((FL[v] + FR[v]) / R(2)) - ((c * (qR[v] - qL[v])) / R(2));
     }
@@ -89,8 +98,8 @@ __device__ __forceinline__ void maxwell_flux(const R* qL, const R* qR, R mu, R e
   }
 }
 
-template <typename Real, int LIM, int RIEM, int COORD, int TY>
-__global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
+template <typename Real, int LIM, int RIEM, int COORD, int TY, int MINB>
+__global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
     maxwell_stage_kernel(const __grid_constant__ CUtensorMap tmap, const MaxwellParams<Real> p) {
   using C = MaxwellCfg<Real, TY>;
   using G = Geo<Real, COORD>;
@@ -120,10 +129,8 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
   }
   __syncthreads();
   unsigned phase_bits = 0, pending = 0;
-  auto U = [&](int pl, int q, int r, int c) -> Real& {
-    return uring[pmod(pl, C::NSLOT) * C::SLOT + q * PL + r * W + c];
-  };
-  auto Rr = [&](int pl, int q, int r, int c) -> Real& { return rring[(pmod(pl, 3) * 2 + q) * PL + r * W + c]; };
+  // ring access through per-step plane bases (no modulo per access)
+  auto UA = [&](const Real* b, int q, int r, int c) -> Real { return b[q * PL + r * W + c]; };
 
   const bool is_out = tid < TX * TY;
   const int otx = tid % TX, oty = tid / TX;
@@ -161,6 +168,12 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
         phase_bits ^= 1u << s;
         pending &= ~(1u << s);
       }
+      const Real* uK = uring + pmod(K, C::NSLOT) * C::SLOT;
+      const Real* uK1 = uring + pmod(K + 1, C::NSLOT) * C::SLOT;
+      const Real* uK2 = uring + pmod(K + 2, C::NSLOT) * C::SLOT;
+      const Real* rKm = rring + pmod(K - 1, 3) * 2 * PL;
+      const Real* rK = rring + pmod(K, 3) * 2 * PL;
+      Real* rK1 = rring + pmod(K + 1, 3) * 2 * PL;
       // cleaning residuals of plane K+1 on interior cells of the tile + 1
       {
         const int pl = K + 1, k = pl - 1;
@@ -169,26 +182,39 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
             const int r = HH - 1 + it / (TX + 2), c = 3 + it % (TX + 2);
             const int i = x0 + c - 4, j = y0 + r - HH;
             if (i < 0 || i >= nx || j < 0 || j >= ny) continue;
-            const Real l1 = G::L1(p.met, i, j, k), l2 = G::L2(p.met, i, j, k), l3 = G::L3(p.met, i, j, k);
             Real div[2];
+            Lame<Real> lm;
+            if constexpr (COORD != COORD_CART) lame_at<Real, COORD>(p.met, i, j, lm);
 #pragma unroll
             for (int f = 0; f < 2; ++f) {
               const int q0 = 3 * f;
-              const Real d1 = (U(pl, q0, r, c + 1) - U(pl, q0, r, c - 1)) / (Real(2) * l1);
-              const Real d2 = (U(pl, q0 + 1, r + 1, c) - U(pl, q0 + 1, r - 1, c)) / (Real(2) * l2);
-              const Real d3 = (U(pl + 1, q0 + 2, r, c) - U(pl - 1, q0 + 2, r, c)) / (Real(2) * l3);
+              Real d1, d2, d3;
+              if constexpr (sizeof(Real) == 4) {
+                d1 = (UA(uK1, q0, r, c + 1) - UA(uK1, q0, r, c - 1)) * (0.5f * inv_len<Real, COORD, 0>(p.met, i, j, k));
+                d2 = (UA(uK1, q0 + 1, r + 1, c) - UA(uK1, q0 + 1, r - 1, c)) * (0.5f * inv_len<Real, COORD, 1>(p.met, i, j, k));
+                d3 = (UA(uK2, q0 + 2, r, c) - UA(uK, q0 + 2, r, c)) * (0.5f * inv_len<Real, COORD, 2>(p.met, i, j, k));
+              } else {
+                const Real l1 = G::L1(p.met, i, j, k), l2 = G::L2(p.met, i, j, k), l3 = G::L3(p.met, i, j, k);
+                d1 = (UA(uK1, q0, r, c + 1) - UA(uK1, q0, r, c - 1)) / (Real(2) * l1);
+                d2 = (UA(uK1, q0 + 1, r + 1, c) - UA(uK1, q0 + 1, r - 1, c)) / (Real(2) * l2);
+                d3 = (UA(uK2, q0 + 2, r, c) - UA(uK, q0 + 2, r, c)) / (Real(2) * l3);
+              }
               Real dv = (d1 + d2) + d3;
               if constexpr (COORD != COORD_CART) {
-                Lame<Real> lm;
-                lame_at<Real, COORD>(p.met, i, j, lm);
-                dv = ((dv + ((U(pl, q0, r, c) * (lm.dl[0][1] + lm.dl[0][2])) / lm.h[0])) +
-                      ((U(pl, q0 + 1, r, c) * (lm.dl[1][0] + lm.dl[1][2])) / lm.h[1])) +
-                     ((U(pl, q0 + 2, r, c) * (lm.dl[2][0] + lm.dl[2][1])) / lm.h[2]);
+                if constexpr (sizeof(Real) == 4) {
+                  dv = ((dv + (UA(uK1, q0, r, c) * (lm.dl[0][1] + lm.dl[0][2])) * recip(lm.h[0])) +
+                        (UA(uK1, q0 + 1, r, c) * (lm.dl[1][0] + lm.dl[1][2])) * recip(lm.h[1])) +
+                       (UA(uK1, q0 + 2, r, c) * (lm.dl[2][0] + lm.dl[2][1])) * recip(lm.h[2]);
+                } else {
+                  dv = ((dv + ((UA(uK1, q0, r, c) * (lm.dl[0][1] + lm.dl[0][2])) / lm.h[0])) +
+                        ((UA(uK1, q0 + 1, r, c) * (lm.dl[1][0] + lm.dl[1][2])) / lm.h[1])) +
+                       ((UA(uK1, q0 + 2, r, c) * (lm.dl[2][0] + lm.dl[2][1])) / lm.h[2]);
+                }
               }
               div[f] = dv;
             }
-            Rr(pl, 0, r, c) = div[0];
-            Rr(pl, 1, r, c) = div[1] - Real(p.rho_c);
+            rK1[r * W + c] = div[0];
+            rK1[PL + r * W + c] = div[1] - Real(p.rho_c);
           }
         }
       }
@@ -197,7 +223,7 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
         const int r = oty + HH, c = otx + 4;
         Real qm[NV], q0[NV], qp[NV], zn[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { qm[v] = U(K, v, r, c); q0[v] = U(K + 1, v, r, c); qp[v] = U(K + 2, v, r, c); }
+        for (int v = 0; v < NV; ++v) { qm[v] = UA(uK, v, r, c); q0[v] = UA(uK1, v, r, c); qp[v] = UA(uK2, v, r, c); }
         const bool ghost = (K + 1 <= 0 || K + 1 >= nz + 1);
         if (ghost || !out_valid) {
 #pragma unroll
@@ -221,6 +247,13 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
       __syncthreads();
       if (K < Z0) continue;
       const int kK = K - 1;
+      if (out_valid && otx == 0) {
+        const long long g0 = L.idx(0, K, oj + 1, oi + 1);
+        for (int v = 0; v < NV; ++v) {
+          if (p.coef.mode >= MODE_AXPY && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
+          if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) prefetch_l2(p.acc + g0 + v * L.var_stride);
+        }
+      }
       // x1 faces
       for (int it = tid; it < TY * (TX + 2); it += NT) {
         const int ty = it / (TX + 2), tx = it % (TX + 2) - 1;
@@ -230,8 +263,8 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
         const int o = ty * (TX + 2) + tx + 1;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-          const Real f0 = U(K, v, r, c);
-          const Real s = interior ? muscl_slope<LIM>(U(K, v, r, c - 1), f0, U(K, v, r, c + 1), l1) : Real(0);
+          const Real f0 = UA(uK, v, r, c);
+          const Real s = interior ? muscl_slope<LIM>(UA(uK, v, r, c - 1), f0, UA(uK, v, r, c + 1), l1) : Real(0);
           fL[v * C::XB + o] = f0 + s / Real(2);
           fR[v * C::XB + o] = f0 - s / Real(2);
         }
@@ -273,8 +306,8 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
         const int o = (ty + 1) * TX + tx;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-          const Real f0 = U(K, v, r, c);
-          const Real s = interior ? muscl_slope<LIM>(U(K, v, r - 1, c), f0, U(K, v, r + 1, c), l2) : Real(0);
+          const Real f0 = UA(uK, v, r, c);
+          const Real s = interior ? muscl_slope<LIM>(UA(uK, v, r - 1, c), f0, UA(uK, v, r + 1, c), l2) : Real(0);
           fL[v * C::XB + o] = f0 + s / Real(2);
           fR[v * C::XB + o] = f0 - s / Real(2);
         }
@@ -303,7 +336,7 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
         const int r = oty + HH, c = otx + 4;
         Real q[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) q[v] = U(K, v, r, c);
+        for (int v = 0; v < NV; ++v) q[v] = UA(uK, v, r, c);
         // geometric source from the cell curl tensors (zero in cartesian)
         Real sg[NV];
 #pragma unroll
@@ -329,14 +362,30 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
         const int im = max(oi - 1, 0) - oi, ip = min(oi + 1, nx - 1) - oi;
         const int jm = max(oj - 1, 0) - oj, jp = min(oj + 1, ny - 1) - oj;
         const int km = (K - 1 >= 1) ? -1 : 0, kp = (K + 1 <= nz) ? 1 : 0;
-        const Real l1 = G::L1(p.met, oi, oj, kK), l2 = G::L2(p.met, oi, oj, kK), l3 = G::L3(p.met, oi, oj, kK);
+        Real h1, h2, h3;  // 1/(2L) (float32) or 2L (float64)
+        if constexpr (sizeof(Real) == 4) {
+          h1 = 0.5f * inv_len<Real, COORD, 0>(p.met, oi, oj, kK);
+          h2 = 0.5f * inv_len<Real, COORD, 1>(p.met, oi, oj, kK);
+          h3 = 0.5f * inv_len<Real, COORD, 2>(p.met, oi, oj, kK);
+        } else {
+          h1 = Real(2) * G::L1(p.met, oi, oj, kK);
+          h2 = Real(2) * G::L2(p.met, oi, oj, kK);
+          h3 = Real(2) * G::L3(p.met, oi, oj, kK);
+        }
+        auto grad = [&](Real d, Real h) -> Real {
+          if constexpr (sizeof(Real) == 4) return d * h;
+          else return d / h;
+        };
         Real sc[NV];
 #pragma unroll
         for (int f = 0; f < 2; ++f) {
           const Real chi = f == 0 ? Real(p.chi_b) : Real(p.chi_d);
-          const Real g1 = (Rr(K, f, r, c + ip) - Rr(K, f, r, c + im)) / (Real(2) * l1);
-          const Real g2 = (Rr(K, f, r + jp, c) - Rr(K, f, r + jm, c)) / (Real(2) * l2);
-          const Real g3 = (Rr(K + kp, f, r, c) - Rr(K + km, f, r, c)) / (Real(2) * l3);
+          const Real* rb = rK + f * PL + r * W + c;
+          const Real* rbp = (kp ? rK1 : rK) + f * PL + r * W + c;
+          const Real* rbm = (km ? rKm : rK) + f * PL + r * W + c;
+          const Real g1 = grad(rb[ip] - rb[im], h1);
+          const Real g2 = grad(rb[jp * W] - rb[jm * W], h2);
+          const Real g3 = grad(rbp[0] - rbm[0], h3);
           sc[3 * f + 0] = (-chi) * g1;
           sc[3 * f + 1] = (-chi) * g2;
           sc[3 * f + 2] = (-chi) * g3;
@@ -349,10 +398,12 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, 1)
           const Real Fym = fb[v * C::FB + oty * TX + otx], Fyp = fb[v * C::FB + (oty + 1) * TX + otx];
           const Real sum = ((((Fxp[v] - Fxm[v]) + Fyp) - Fym) + Fzn[v]) - Fzp[v];
           const Real sp = v < 3 ? Real(0) : (-Real(p.sigma)) * (q[v] / ep);
-          const Real k = (-sum) / Vc + ((sg[v] + sp) + sc[v]);
+          Real k;
+          if constexpr (sizeof(Real) == 4) k = (-sum) * rcp_approx(Vc) + ((sg[v] + sp) + sc[v]);
+          else k = (-sum) / Vc + ((sg[v] + sp) + sc[v]);
           const long long gi = gidx + (long long)v * L.var_stride;
           Real u0v = Real(0), accv = Real(0);
-          if (p.coef.mode >= MODE_AXPY) u0v = p.u0[gi];
+          if (p.coef.mode >= MODE_AXPY) u0v = p.coef.u0_is_input ? q[v] : p.u0[gi];
           if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
           const Real o = stage_combine(p.coef, dt, k, q[v], u0v, accv);
           p.out[gi] = o;

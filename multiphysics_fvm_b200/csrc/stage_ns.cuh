@@ -167,19 +167,13 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
   unsigned phase_bits = 0;  // expected parity per slot (identical in all threads)
   unsigned pending = 0;     // slots with a load in flight (meaningful in thread 0)
 
-  // ring accessors: U/v in tile+HH coordinates (r, c), P/tau in tile+2 (r2, c2)
-  auto U = [&](int slot, int q, int r, int c) -> Real& { return uring[slot * C::SLOT + q * PL + r * W + c]; };
-  auto Vv = [&](int pl, int q, int r, int c) -> Real& { return vring[(pmod(pl, 3) * 3 + q) * PL + r * W + c]; };
-  auto Pp = [&](int pl, int r2, int c2) -> Real& { return pring[pmod(pl, 3) * PL2 + r2 * W2 + c2]; };
-  auto Tt = [&](int pl, int q, int r2, int c2) -> Real& {
-    return tring[(pmod(pl, 3) * 6 + q) * PL2 + r2 * W2 + c2];
-  };
-  // value of recon field f (U 0..4, P 5, tau row-d component 6..8) of plane K
-  // at tile offset (tx, ty); ti = tau indices of the row of the face axis
-  auto field = [&](int sK, int K, const int* ti, int f, int tx, int ty) -> Real {
-    if (f < 5) return U(sK, f, ty + HH, tx + 4);
-    if (f == 5) return Pp(K, ty + 2, tx + 2);
-    return Tt(K, ti[f - 6], ty + 2, tx + 2);
+  // Value of recon field f (U 0..4, P 5, tau row-d component 6..8) at tile
+  // offset (tx, ty) of one plane, given that plane's ring bases (computed once
+  // per step); ti = tau indices of the row of the face axis.
+  auto field = [&](const Real* ub, const Real* pb, const Real* tb, const int* ti, int f, int tx, int ty) -> Real {
+    if (f < 5) return ub[f * PL + (ty + HH) * W + tx + 4];
+    if (f == 5) return pb[(ty + 2) * W2 + tx + 2];
+    return tb[ti[f - 6] * PL2 + (ty + 2) * W2 + tx + 2];
   };
 
   const bool is_out = tid < TX * TY;
@@ -237,23 +231,43 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
           for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= K + HH; ++pl) pending &= ~(1u << pmod(pl, C::NSLOT));
       }
       const int sK = pmod(K, C::NSLOT), sK1 = pmod(K + 1, C::NSLOT), sK2 = pmod(K + 2, C::NSLOT);
+      // ring bases of planes K, K+1, K+2 (uniform, once per step)
+      const Real* uK = uring + sK * C::SLOT;
+      const Real* uK1 = uring + sK1 * C::SLOT;
+      const Real* uK2 = uring + sK2 * C::SLOT;
+      const Real* pK = pring + pmod(K, 3) * PL2;
+      const Real* pK1 = pring + pmod(K + 1, 3) * PL2;
+      const Real* pK2 = pring + pmod(K + 2, 3) * PL2;
+      const Real* tK = tring + pmod(K, 3) * 6 * PL2;
+      const Real* tK1 = tring + pmod(K + 1, 3) * 6 * PL2;
+      const Real* tK2 = tring + pmod(K + 2, 3) * 6 * PL2;
+      // lane 0 of each output row asks L2 for this plane's U0/acc rows
+      if (K >= Z0 && out_valid && otx == 0) {
+        const long long g0 = L.idx(0, K, oj + 1, oi + 1);
+        for (int v = 0; v < 5; ++v) {
+          if (p.coef.mode >= MODE_AXPY && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
+          if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) prefetch_l2(p.acc + g0 + v * L.var_stride);
+        }
+      }
       // ---------------------------------------------------------- B ----
       // v on the newest plane(s), tile + 3 (viscous only)
       if constexpr (VISC) {
         for (int pl = (K == Kfirst ? Pfirst : K + 3); pl <= K + 3; ++pl) {
-          const int s = pmod(pl, C::NSLOT);
+          const Real* ub = uring + pmod(pl, C::NSLOT) * C::SLOT;
+          Real* vb = vring + pmod(pl, 3) * 3 * PL;
           for (int it = tid; it < C::ROWS * (TX + 6); it += NT) {
             const int r = it / (TX + 6), c = 1 + it % (TX + 6);
-            const Real rho = U(s, 0, r, c);
+            const int o = r * W + c;
+            const Real rho = ub[o];
             if constexpr (F32) {
               const Real ir = rcp_approx(rho);
-              Vv(pl, 0, r, c) = U(s, 1, r, c) * ir;
-              Vv(pl, 1, r, c) = U(s, 2, r, c) * ir;
-              Vv(pl, 2, r, c) = U(s, 3, r, c) * ir;
+              vb[o] = ub[PL + o] * ir;
+              vb[PL + o] = ub[2 * PL + o] * ir;
+              vb[2 * PL + o] = ub[3 * PL + o] * ir;
             } else {
-              Vv(pl, 0, r, c) = U(s, 1, r, c) / rho;
-              Vv(pl, 1, r, c) = U(s, 2, r, c) / rho;
-              Vv(pl, 2, r, c) = U(s, 3, r, c) / rho;
+              vb[o] = ub[PL + o] / rho;
+              vb[PL + o] = ub[2 * PL + o] / rho;
+              vb[2 * PL + o] = ub[3 * PL + o] / rho;
             }
           }
         }
@@ -261,21 +275,21 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       // ---------------------------------------------------------- C ----
       // P on plane K+2, tile + 2 (navier_stokes.py:94-100)
       {
-        const int pl = K + 2;
+        Real* pw = pring + pmod(K + 2, 3) * PL2;
         for (int it = tid; it < C::PL2; it += NT) {
           const int r2 = it / W2, c2 = it % W2;
-          const int r = r2 + HH - 2, c = c2 + 2;
-          const Real rho = U(sK2, 0, r, c);
+          const Real* u = uK2 + (r2 + HH - 2) * W + c2 + 2;
+          const Real rho = u[0];
           Real v0, v1, v2, E;
           if constexpr (F32) {
             const Real ir = rcp_approx(rho);
-            v0 = U(sK2, 1, r, c) * ir; v1 = U(sK2, 2, r, c) * ir; v2 = U(sK2, 3, r, c) * ir;
-            E = U(sK2, 4, r, c) * ir;
+            v0 = u[PL] * ir; v1 = u[2 * PL] * ir; v2 = u[3 * PL] * ir;
+            E = u[4 * PL] * ir;
           } else {
-            v0 = U(sK2, 1, r, c) / rho; v1 = U(sK2, 2, r, c) / rho; v2 = U(sK2, 3, r, c) / rho;
-            E = U(sK2, 4, r, c) / rho;
+            v0 = u[PL] / rho; v1 = u[2 * PL] / rho; v2 = u[3 * PL] / rho;
+            E = u[4 * PL] / rho;
           }
-          Pp(pl, r2, c2) = ((gam - Real(1)) * rho) * (E - (((v0 * v0) + (v1 * v1)) + (v2 * v2)) / Real(2));
+          pw[it] = ((gam - Real(1)) * rho) * (E - (((v0 * v0) + (v1 * v1)) + (v2 * v2)) / Real(2));
         }
       }
       if constexpr (VISC) __syncthreads();
@@ -285,6 +299,10 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         const int pl = K + 2;
         const int k = pl - 1;  // interior plane index
         const bool zghost = (k < 0 || k >= nz);
+        const Real* vm = vring + pmod(pl - 1, 3) * 3 * PL;  // v of planes K+1, K+2, K+3
+        const Real* v0p = vring + pmod(pl, 3) * 3 * PL;
+        const Real* vp = vring + pmod(pl + 1, 3) * 3 * PL;
+        Real* tw = tring + pmod(pl, 3) * 6 * PL2;
         for (int it = tid; it < C::PL2; it += NT) {
           const int r2 = it / W2, c2 = it % W2;
           const int r = r2 + 1, c = c2 + 2;
@@ -301,17 +319,19 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
               const Real h3 = 0.5f * inv_len<Real, COORD, 2>(p.met, i, j, k);
 #pragma unroll
               for (int cc = 0; cc < 3; ++cc) {
-                g[cc][0] = (Vv(pl, cc, r, c + 1) - Vv(pl, cc, r, c - 1)) * h1;
-                g[cc][1] = (Vv(pl, cc, r + 1, c) - Vv(pl, cc, r - 1, c)) * h2;
-                g[cc][2] = (Vv(pl + 1, cc, r, c) - Vv(pl - 1, cc, r, c)) * h3;
+                const int o = cc * PL + r * W + c;
+                g[cc][0] = (v0p[o + 1] - v0p[o - 1]) * h1;
+                g[cc][1] = (v0p[o + W] - v0p[o - W]) * h2;
+                g[cc][2] = (vp[o] - vm[o]) * h3;
               }
             } else {
               const Real l1 = G::L1(p.met, i, j, k), l2 = G::L2(p.met, i, j, k), l3 = G::L3(p.met, i, j, k);
 #pragma unroll
               for (int cc = 0; cc < 3; ++cc) {
-                g[cc][0] = (Vv(pl, cc, r, c + 1) - Vv(pl, cc, r, c - 1)) / (Real(2) * l1);
-                g[cc][1] = (Vv(pl, cc, r + 1, c) - Vv(pl, cc, r - 1, c)) / (Real(2) * l2);
-                g[cc][2] = (Vv(pl + 1, cc, r, c) - Vv(pl - 1, cc, r, c)) / (Real(2) * l3);
+                const int o = cc * PL + r * W + c;
+                g[cc][0] = (v0p[o + 1] - v0p[o - 1]) / (Real(2) * l1);
+                g[cc][1] = (v0p[o + W] - v0p[o - W]) / (Real(2) * l2);
+                g[cc][2] = (vp[o] - vm[o]) / (Real(2) * l3);
               }
             }
             const Real tt = Real(2.0 / 3.0);
@@ -326,7 +346,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
             } else {
               Lame<Real> lm;
               lame_at<Real, COORD>(p.met, i, j, lm);
-              const Real v0 = Vv(pl, 0, r, c), v1 = Vv(pl, 1, r, c), v2 = Vv(pl, 2, r, c);
+              const Real v0 = v0p[r * W + c], v1 = v0p[PL + r * W + c], v2 = v0p[2 * PL + r * W + c];
               const Real divv = (((((g[0][0] + g[1][1]) + g[2][2]) + ((v0 * (lm.dl[0][1] + lm.dl[0][2])) / lm.h[0])) +
                                   ((v1 * (lm.dl[1][0] + lm.dl[1][2])) / lm.h[1])) +
                                  ((v2 * (lm.dl[2][0] + lm.dl[2][1])) / lm.h[2]));
@@ -340,7 +360,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
             }
           }
 #pragma unroll
-          for (int m = 0; m < 6; ++m) Tt(pl, m, r2, c2) = t[m];
+          for (int m = 0; m < 6; ++m) tw[m * PL2 + it] = t[m];
         }
       }
       __syncthreads();
@@ -355,9 +375,9 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         Real qm[NREC], q0[NREC], qp[NREC];
 #pragma unroll
         for (int f = 0; f < NREC; ++f) {
-          qm[f] = field(sK, K, ti, f, otx, oty);
-          q0[f] = field(sK1, K + 1, ti, f, otx, oty);
-          qp[f] = field(sK2, K + 2, ti, f, otx, oty);
+          qm[f] = field(uK, pK, tK, ti, f, otx, oty);
+          q0[f] = field(uK1, pK1, tK1, ti, f, otx, oty);
+          qp[f] = field(uK2, pK2, tK2, ti, f, otx, oty);
         }
         if (ghost || !out_valid) {
 #pragma unroll
@@ -393,8 +413,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
           const Real l1 = (F32 || !interior) ? Real(1) : G::L1(p.met, i, j, kK);
 #pragma unroll
           for (int f = 0; f < NREC; ++f) {
-            const Real s = interior ? muscl_slope<LIM>(field(sK, K, ti, f, tx - 1, ty), field(sK, K, ti, f, tx, ty),
-                                                       field(sK, K, ti, f, tx + 1, ty), l1)
+            const Real s = interior ? muscl_slope<LIM>(field(uK, pK, tK, ti, f, tx - 1, ty), field(uK, pK, tK, ti, f, tx, ty),
+                                                       field(uK, pK, tK, ti, f, tx + 1, ty), l1)
                                     : Real(0);
             sl[f * C::XB + it] = s;
           }
@@ -412,8 +432,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
             const int oL = ty * (TX + 2) + fx;  // slope slot of the left cell (tx = fx-1)
 #pragma unroll
             for (int f = 0; f < NREC; ++f) {
-              qL[f] = field(sK, K, ti, f, fx - 1, ty) + sl[f * C::XB + oL] / Real(2);
-              qR[f] = field(sK, K, ti, f, fx, ty) - sl[f * C::XB + oL + 1] / Real(2);
+              qL[f] = field(uK, pK, tK, ti, f, fx - 1, ty) + sl[f * C::XB + oL] / Real(2);
+              qR[f] = field(uK, pK, tK, ti, f, fx, ty) - sl[f * C::XB + oL + 1] / Real(2);
             }
             ns_flux<Real, 0, RIEM, VISC>(qL, qR, gam, F);
             const Real s1 = G::S1(p.met, fi, j, kK);
@@ -443,8 +463,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
           const Real l2 = (F32 || !interior) ? Real(1) : G::L2(p.met, i, j, kK);
 #pragma unroll
           for (int f = 0; f < NREC; ++f) {
-            const Real s = interior ? muscl_slope<LIM>(field(sK, K, ti, f, tx, ty - 1), field(sK, K, ti, f, tx, ty),
-                                                       field(sK, K, ti, f, tx, ty + 1), l2)
+            const Real s = interior ? muscl_slope<LIM>(field(uK, pK, tK, ti, f, tx, ty - 1), field(uK, pK, tK, ti, f, tx, ty),
+                                                       field(uK, pK, tK, ti, f, tx, ty + 1), l2)
                                     : Real(0);
             sl[f * C::XB + it] = s;
           }
@@ -462,8 +482,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
             const int oL = fy * TX + tx;  // slope slot of the lower cell (ty = fy-1)
 #pragma unroll
             for (int f = 0; f < NREC; ++f) {
-              qL[f] = field(sK, K, ti, f, tx, fy - 1) + sl[f * C::XB + oL] / Real(2);
-              qR[f] = field(sK, K, ti, f, tx, fy) - sl[f * C::XB + oL + TX] / Real(2);
+              qL[f] = field(uK, pK, tK, ti, f, tx, fy - 1) + sl[f * C::XB + oL] / Real(2);
+              qR[f] = field(uK, pK, tK, ti, f, tx, fy) - sl[f * C::XB + oL + TX] / Real(2);
             }
             ns_flux<Real, 1, RIEM, VISC>(qL, qR, gam, F);
             const Real s2 = G::S2(p.met, i, fj, kK);
@@ -480,7 +500,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         const int r = oty + HH, c = otx + 4;
         Real q[5];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) q[v] = U(sK, v, r, c);
+        for (int v = 0; v < 5; ++v) q[v] = uK[v * PL + r * W + c];
         const Real rho = q[0];
         Real v0, v1, v2;
         if constexpr (F32) {
@@ -500,15 +520,16 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         if constexpr (COORD != COORD_CART) {
           Lame<Real> lm;
           lame_at<Real, COORD>(p.met, oi, oj, lm);
-          const Real P = Pp(K, oty + 2, otx + 2);
+          const Real P = pK[(oty + 2) * W2 + otx + 2];
           const Real vv[3] = {v0, v1, v2};
           Real tc[3][3];
           if constexpr (VISC) {
             const int r2 = oty + 2, c2 = otx + 2;
-            tc[0][0] = Tt(K, 0, r2, c2); tc[1][1] = Tt(K, 1, r2, c2); tc[2][2] = Tt(K, 2, r2, c2);
-            tc[0][1] = tc[1][0] = Tt(K, 3, r2, c2);
-            tc[0][2] = tc[2][0] = Tt(K, 4, r2, c2);
-            tc[1][2] = tc[2][1] = Tt(K, 5, r2, c2);
+            const Real* tc0 = tK + r2 * W2 + c2;
+            tc[0][0] = tc0[0]; tc[1][1] = tc0[PL2]; tc[2][2] = tc0[2 * PL2];
+            tc[0][1] = tc[1][0] = tc0[3 * PL2];
+            tc[0][2] = tc[2][0] = tc0[4 * PL2];
+            tc[1][2] = tc[2][1] = tc0[5 * PL2];
           } else {
 #pragma unroll
             for (int a = 0; a < 3; ++a)
@@ -542,7 +563,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
           else k = (-sum) / Vc + src[v];
           const long long gi = gidx + (long long)v * L.var_stride;
           Real u0v = Real(0), accv = Real(0);
-          if (p.coef.mode >= MODE_AXPY) u0v = p.u0[gi];
+          if (p.coef.mode >= MODE_AXPY) u0v = p.coef.u0_is_input ? q[v] : p.u0[gi];
           if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
           const Real o = stage_combine(p.coef, dt, k, q[v], u0v, accv);
           p.out[gi] = o;
