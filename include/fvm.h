@@ -146,6 +146,26 @@ int fvm_clear_status(fvm_handle* h);
 int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_kernel_ms,
                       double* other_kernel_ms, int* stage_launches);
 
+/* Pick the z-march depth (planes per tile) by timing the candidates on this grid;
+ * the state and clock are restored afterwards.  New: the reference has no tuning. */
+int fvm_autotune(fvm_handle* h, int* best_zchunk, double* best_ms_per_step);
+
+/* ---- batches of independent grids (SURVEY configuration C3) -------------------
+ * Many setups of uneven sizes advance together: one persistent launch per kernel
+ * specialisation and stage walks a flat tile list over all grids, and every grid
+ * keeps its own CFL time step.  All grids share the time integrator and the
+ * precision; navier_stokes and heat grids may be mixed.  Each grid is an ordinary
+ * handle (fvm_batch_handle) for upload/download/set_time/get_time/totals.
+ * Replaces n independent solver.run loops (src/solver.py:88-151). */
+typedef struct fvm_batch fvm_batch;
+int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out);
+int fvm_batch_destroy(fvm_batch* b);
+int fvm_batch_size(const fvm_batch* b, int* n, long long* tiles);
+int fvm_batch_handle(fvm_batch* b, int i, fvm_handle** h);
+int fvm_batch_step(fvm_batch* b, int n_steps, int dt_mode);
+int fvm_batch_time_steps(fvm_batch* b, int n_steps, int dt_mode, double* ms);
+int fvm_batch_autotune(fvm_batch* b, int* best_zchunk, double* best_ms_per_step);
+
 /* Conserved totals sum_q(cells[q][i] * volumes[i]) in float64 with compensated
  * summation, computed without allocating any device memory.  No counterpart in
  * the reference.  For callers that cannot call cudaMalloc (a host framework

@@ -109,6 +109,14 @@ class Simulation:
                  space_schemes: dict, bcs: dict, integrator=None, precision: str = "fp64",
                  zchunk: int = 0, tile_ty: int = 0):
         lib = L.load()
+        d = self._describe(physics, coordinate_system, grid_config, params, space_schemes, bcs, integrator,
+                           precision, zchunk, tile_ty)
+        h = C.c_void_p()
+        L.check(lib.fvm_create(C.byref(d), C.byref(h)), "fvm_create")
+        self._attach(h, lib, owned=True)
+
+    def _describe(self, physics, coordinate_system, grid_config, params, space_schemes, bcs, integrator,
+                  precision, zchunk, tile_ty):
         self.physics = physics
         self.nv = len(VARIABLES[physics])
         self.variables = VARIABLES[physics]
@@ -144,17 +152,19 @@ class Simulation:
         d.tile_ty = int(tile_ty)
         self.desc = d
         self.precision = precision
-        h = C.c_void_p()
-        L.check(lib.fvm_create(C.byref(d), C.byref(h)), "fvm_create")
+        return d
+
+    def _attach(self, h, lib, owned):
         self._h = h
         self._lib = lib
+        self._owned = owned
         self._ghosted = (self.nv,) + tuple(x + 2 for x in self.n)
 
     # -- life cycle --------------------------------------------------------
     def close(self):
-        if getattr(self, "_h", None) is not None and self._h.value:
+        if getattr(self, "_h", None) is not None and self._h.value and getattr(self, "_owned", True):
             self._lib.fvm_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
@@ -245,10 +255,79 @@ class Simulation:
     def clear_status(self):
         L.check(self._lib.fvm_clear_status(self._h), "fvm_clear_status")
 
+    def autotune(self):
+        """Choose the z-march depth by timing candidates (state restored); returns (zchunk, ms/step)."""
+        z, ms = C.c_int(), C.c_double()
+        L.check(self._lib.fvm_autotune(self._h, C.byref(z), C.byref(ms)), "fvm_autotune")
+        return z.value, ms.value
+
     def info(self):
         nv, nb = C.c_int(), C.c_longlong()
         L.check(self._lib.fvm_info(self._h, C.byref(nv), C.byref(nb)), "fvm_info")
         return nv.value, nb.value
+
+
+class Batch:
+    """Independent grids advanced together by one persistent launch per kernel
+    specialisation and stage (``fvm_batch_*``); each grid keeps its own CFL dt.
+    ``setups`` are setup dicts (same integrator and precision; navier_stokes and
+    heat may be mixed).  ``batch[i]`` is the i-th grid as a Simulation view."""
+
+    def __init__(self, setups):
+        lib = L.load()
+        descs = (L.FvmDesc * len(setups))()
+        self.sims = []
+        for i, s in enumerate(setups):
+            sim = Simulation.__new__(Simulation)
+            descs[i] = sim._describe(physics_name(s["physics"]), s["coordinate_system"], s["grid_config"],
+                                     s["physical_parameters"], s["space_schemes"], s["boundary_conditions"],
+                                     s.get("time_integrator"), s.get("precision", "fp64"), 0, 0)
+            self.sims.append(sim)
+        b = C.c_void_p()
+        L.check(lib.fvm_batch_create(descs, len(setups), C.byref(b)), "fvm_batch_create")
+        self._b, self._lib = b, lib
+        for i, sim in enumerate(self.sims):
+            h = C.c_void_p()
+            L.check(lib.fvm_batch_handle(b, i, C.byref(h)), "fvm_batch_handle")
+            sim._attach(h, lib, owned=False)
+
+    def __len__(self):
+        return len(self.sims)
+
+    def __getitem__(self, i) -> Simulation:
+        return self.sims[i]
+
+    def tiles(self) -> int:
+        n, t = C.c_int(), C.c_longlong()
+        L.check(self._lib.fvm_batch_size(self._b, C.byref(n), C.byref(t)), "fvm_batch_size")
+        return t.value
+
+    def step(self, n_steps: int = 1, fixed_dt: bool = False):
+        L.check(self._lib.fvm_batch_step(self._b, int(n_steps), 1 if fixed_dt else 0), "fvm_batch_step")
+
+    def time_steps(self, n_steps: int, fixed_dt: bool = False) -> float:
+        ms = C.c_double()
+        L.check(self._lib.fvm_batch_time_steps(self._b, int(n_steps), 1 if fixed_dt else 0, C.byref(ms)),
+                "fvm_batch_time_steps")
+        return ms.value
+
+    def autotune(self):
+        z, ms = C.c_int(), C.c_double()
+        L.check(self._lib.fvm_batch_autotune(self._b, C.byref(z), C.byref(ms)), "fvm_batch_autotune")
+        return z.value, ms.value
+
+    def close(self):
+        if getattr(self, "_b", None) is not None and self._b.value:
+            for s in self.sims:
+                s._h = None
+            self._lib.fvm_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class _Cache:

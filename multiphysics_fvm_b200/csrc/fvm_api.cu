@@ -247,19 +247,51 @@ void fill_common(fvm_handle* h, const StageDef& sd, bool rhs_only, P& p) {
   p.zchunk = h->zchunk;
 }
 
+// x3 fluxes cancel exactly on a one-plane grid whose x3 ghosts copy the plane
+// (periodic or Neumann for every variable): the float32 inviscid path then
+// skips the x3 pipeline ("flat").
+bool flat_grid(const fvm_handle* h) {
+  const fvm_desc& d = h->d;
+  if (h->f64 || d.nx3 != 1 || d.physics != FVM_NAVIER_STOKES || d.params[1] != 0.0) return false;
+  for (int q = 0; q < h->nv; ++q)
+    for (int s = 4; s < 6; ++s)
+      if (d.bc_kind[q][s] != FVM_BC_PERIODIC && d.bc_kind[q][s] != FVM_BC_NEUMANN) return false;
+  return true;
+}
+
+template <typename Real>
+NsParams<Real> make_ns_params(fvm_handle* h, const StageDef& sd, bool rhs_only) {
+  const fvm_desc& d = h->d;
+  NsParams<Real> p{};
+  fill_common<Real>(h, sd, rhs_only, p);
+  p.gamma = d.params[0];
+  p.mu = d.params[1];
+  p.g1 = d.params[2];
+  p.g2 = d.params[3];
+  p.g3 = d.params[4];
+  p.flat = (!rhs_only && flat_grid(h)) ? 1 : 0;
+  return p;
+}
+
+template <typename Real>
+HeatParams<Real> make_heat_params(fvm_handle* h, const StageDef& sd, bool rhs_only) {
+  const fvm_desc& d = h->d;
+  HeatParams<Real> p{};
+  fill_common<Real>(h, sd, rhs_only, p);
+  p.rho_cp = d.params[0] * d.params[1];
+  p.inv_rho_cp = 1.0 / (d.params[0] * d.params[1]);
+  p.k = d.params[2];
+  p.q = d.params[3];
+  return p;
+}
+
 template <typename Real>
 cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool prepare_only = false) {
   const fvm_desc& d = h->d;
   const int nsm = prepare_only ? -1 : h->nsm;
-  if (d.physics == FVM_HEAT) {
-    HeatParams<Real> p{};
-    fill_common<Real>(h, sd, rhs_only, p);
-    p.rho_cp = d.params[0] * d.params[1];
-    p.inv_rho_cp = 1.0 / (d.params[0] * d.params[1]);
-    p.k = d.params[2];
-    p.q = d.params[3];
-    return launch_heat<Real>(kernel_limiter(d), d.coords, h->tmap[sd.in], p, h->stream, nsm);
-  }
+  if (d.physics == FVM_HEAT)
+    return launch_heat<Real>(kernel_limiter(d), d.coords, h->tmap[sd.in], make_heat_params<Real>(h, sd, rhs_only),
+                             h->stream, nsm);
   if (d.physics == FVM_MAXWELL) {
     MaxwellParams<Real> p{};
     fill_common<Real>(h, sd, rhs_only, p);
@@ -272,30 +304,9 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
     p.c = 1 / std::sqrt(d.params[0] * d.params[1]);
     return launch_maxwell<Real>(kernel_limiter(d), d.riemann, d.coords, h->tmap[sd.in], p, h->stream, nsm);
   }
-  NsParams<Real> p{};
-  p.lay = h->lay;
-  p.met = metric_ptrs<Real>(static_cast<const Real*>(h->met_real), d);
-  p.u0 = static_cast<const Real*>(h->U[0]);
-  p.out = static_cast<Real*>(h->U[sd.out]);
-  p.acc = static_cast<Real*>(h->acc);
-  p.dt = &h->clk->dt;
-  p.active = rhs_only ? nullptr : &h->clk->active;
-  p.coef.mode = sd.mode;
-  p.coef.accmode = sd.accmode;
-  p.coef.ca = sd.ca;
-  p.coef.cb = sd.cb;
-  p.coef.wacc = sd.w;
-  p.coef.u0_is_input = sd.in == 0 ? 1 : 0;
-  p.gamma = d.params[0];
-  p.mu = d.params[1];
-  p.g1 = d.params[2];
-  p.g2 = d.params[3];
-  p.g3 = d.params[4];
-  p.status = h->status;
-  p.zchunk = h->zchunk;
   const bool visc = d.params[1] != 0.0;
-  return launch_ns<Real>(kernel_limiter(d), d.riemann, d.coords, visc, h->tmap[sd.in], p, h->stream,
-                         prepare_only ? -1 : h->nsm);
+  return launch_ns<Real>(kernel_limiter(d), d.riemann, d.coords, visc, h->tmap[sd.in],
+                         make_ns_params<Real>(h, sd, rhs_only), h->stream, nsm);
 }
 
 cudaError_t launch_bc(fvm_handle* h, int b, bool use_active) {
@@ -861,3 +872,441 @@ extern "C" int fvm_totals_noalloc(const float* cells, const double* volumes, int
   FVM_CK(cudaGetLastError());
   return FVM_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batches of independent grids advanced together (one persistent launch per
+// kernel specialisation and stage, a flat tile list over all grids, each grid
+// with its own CFL time step).
+struct fvm_batch {
+  std::vector<fvm_handle*> h;
+  int integrator = 0, nsm = 148;
+  bool f64 = false;
+  cudaStream_t stream = nullptr;
+  struct Group {
+    int physics = 0, lim = 0, riem = 0, coords = 0;
+    bool visc = false;
+    std::vector<int> members;
+    std::vector<void*> prm;           // device params array per stage
+    std::vector<CUtensorMap*> maps;   // device tensor-map array per stage
+    int* tile_start = nullptr;
+    long long ntiles = 0;
+  };
+  std::vector<Group> groups;
+  BatchAux* aux = nullptr;
+  long long faces = 0;
+  struct DtGroup {
+    int coords = 0;
+    BatchDt* d = nullptr;
+    int n = 0;
+  };
+  std::vector<DtGroup> dtg;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+template <typename Real>
+int build_group_arrays(fvm_batch* b, fvm_batch::Group& g) {
+  const std::vector<StageDef> st = stage_table(b->integrator);
+  for (void* x : g.prm) cudaFree(x);
+  for (CUtensorMap* x : g.maps) cudaFree(x);
+  if (g.tile_start) cudaFree(g.tile_start);
+  g.prm.clear();
+  g.maps.clear();
+  g.tile_start = nullptr;
+  std::vector<int> starts(1, 0);
+  for (size_t si = 0; si < st.size(); ++si) {
+    std::vector<CUtensorMap> maps;
+    void* dev = nullptr;
+    if (g.physics == FVM_NAVIER_STOKES) {
+      std::vector<NsParams<Real>> ps;
+      for (int i : g.members) {
+        NsParams<Real> p = make_ns_params<Real>(b->h[i], st[si], false);
+        if (g.visc) ns_tile_counts<Real, true>(p);
+        else ns_tile_counts<Real, false>(p);
+        ps.push_back(p);
+        maps.push_back(b->h[i]->tmap[st[si].in]);
+        if (si == 0) starts.push_back(starts.back() + p.ntx * p.nty * p.nzc);
+      }
+      FVM_CK(cudaMalloc(&dev, ps.size() * sizeof(ps[0])));
+      FVM_CK(cudaMemcpy(dev, ps.data(), ps.size() * sizeof(ps[0]), cudaMemcpyHostToDevice));
+    } else {
+      std::vector<HeatParams<Real>> ps;
+      for (int i : g.members) {
+        HeatParams<Real> p = make_heat_params<Real>(b->h[i], st[si], false);
+        heat_tile_counts(p);
+        ps.push_back(p);
+        maps.push_back(b->h[i]->tmap[st[si].in]);
+        if (si == 0) starts.push_back(starts.back() + p.ntx * p.nty * p.nzc);
+      }
+      FVM_CK(cudaMalloc(&dev, ps.size() * sizeof(ps[0])));
+      FVM_CK(cudaMemcpy(dev, ps.data(), ps.size() * sizeof(ps[0]), cudaMemcpyHostToDevice));
+    }
+    g.prm.push_back(dev);
+    CUtensorMap* dm = nullptr;
+    FVM_CK(cudaMalloc(&dm, maps.size() * sizeof(CUtensorMap)));
+    FVM_CK(cudaMemcpy(dm, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    g.maps.push_back(dm);
+  }
+  g.ntiles = starts.back();
+  FVM_CK(cudaMalloc(&g.tile_start, starts.size() * sizeof(int)));
+  FVM_CK(cudaMemcpy(g.tile_start, starts.data(), starts.size() * sizeof(int), cudaMemcpyHostToDevice));
+  return FVM_OK;
+}
+
+template <typename Real>
+cudaError_t launch_group_stage(fvm_batch* b, fvm_batch::Group& g, int si, int nsm) {
+  if (g.physics == FVM_NAVIER_STOKES) {
+    BatchSource<NsParams<Real>> src{static_cast<const NsParams<Real>*>(g.prm[si]), g.maps[si], g.tile_start,
+                                    (int)g.members.size()};
+    return launch_ns_batch<Real>(g.lim, g.riem, g.coords, g.visc, src, g.ntiles, b->stream, nsm);
+  }
+  BatchSource<HeatParams<Real>> src{static_cast<const HeatParams<Real>*>(g.prm[si]), g.maps[si], g.tile_start,
+                                    (int)g.members.size()};
+  return launch_heat_batch<Real>(g.lim, g.coords, src, g.ntiles, b->stream, nsm);
+}
+
+int enqueue_batch_step(fvm_batch* b, int dt_mode) {
+  const int n = (int)b->h.size();
+  if (dt_mode == 0) {
+    for (auto& dg : b->dtg) {
+      dim3 grid(32, dg.n);
+#define FVM_BDT(R, C) batch_ns_dt_kernel<R, C><<<grid, 256, 0, b->stream>>>(dg.d)
+      if (b->f64) {
+        if (dg.coords == FVM_CARTESIAN) FVM_BDT(double, COORD_CART);
+        else if (dg.coords == FVM_CYLINDRICAL) FVM_BDT(double, COORD_CYL);
+        else FVM_BDT(double, COORD_SPH);
+      } else {
+        if (dg.coords == FVM_CARTESIAN) FVM_BDT(float, COORD_CART);
+        else if (dg.coords == FVM_CYLINDRICAL) FVM_BDT(float, COORD_CYL);
+        else FVM_BDT(float, COORD_SPH);
+      }
+#undef FVM_BDT
+      FVM_CK(cudaGetLastError());
+    }
+  }
+  batch_clock_kernel<<<(n + 127) / 128, 128, 0, b->stream>>>(b->aux, n, dt_mode == 1 ? 1 : 0);
+  FVM_CK(cudaGetLastError());
+  const std::vector<StageDef> st = stage_table(b->integrator);
+  const int bcb = (int)std::min<long long>((b->faces + 255) / 256, 8192);
+  for (size_t si = 0; si < st.size(); ++si) {
+    if (b->f64) batch_bc_kernel<double><<<bcb, 256, 0, b->stream>>>(b->aux, n, b->faces, st[si].in);
+    else batch_bc_kernel<float><<<bcb, 256, 0, b->stream>>>(b->aux, n, b->faces, st[si].in);
+    FVM_CK(cudaGetLastError());
+    for (auto& g : b->groups) {
+      cudaError_t e = b->f64 ? launch_group_stage<double>(b, g, (int)si, b->nsm)
+                             : launch_group_stage<float>(b, g, (int)si, b->nsm);
+      if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("batched stage kernel: ") + cudaGetErrorString(e));
+    }
+  }
+  if (b->integrator == FVM_EULER_EXPLICIT)
+    for (fvm_handle* h : b->h)
+      FVM_CK(cudaMemcpyAsync(h->U[0], h->U[1], h->lay.var_stride * h->nv * h->esz, cudaMemcpyDeviceToDevice,
+                             b->stream));
+  return FVM_OK;
+}
+
+int batch_prepare(fvm_batch* b) {
+  for (auto& g : b->groups) {
+    cudaError_t e = b->f64 ? launch_group_stage<double>(b, g, 0, -1) : launch_group_stage<float>(b, g, 0, -1);
+    FVM_CK(e);
+  }
+  return FVM_OK;
+}
+
+int batch_graph(fvm_batch* b, int dt_mode) {
+  cudaGraphExec_t& ge = b->graph[dt_mode];
+  if (ge) return FVM_OK;
+  int rc = batch_prepare(b);
+  if (rc) return rc;
+  for (fvm_handle* h : b->h) FVM_CK(cudaStreamSynchronize(h->stream));
+  cudaGraph_t g;
+  FVM_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  rc = enqueue_batch_step(b, dt_mode);
+  cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+  if (rc) return rc;
+  FVM_CK(ce);
+  ce = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  FVM_CK(ce);
+  return FVM_OK;
+}
+
+void batch_drop_graphs(fvm_batch* b) {
+  for (auto& g : b->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+}  // namespace
+
+extern "C" {
+
+int fvm_batch_destroy(fvm_batch* b) {
+  if (!b) return FVM_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_drop_graphs(b);
+  for (auto& g : b->groups) {
+    for (void* x : g.prm) cudaFree(x);
+    for (CUtensorMap* x : g.maps) cudaFree(x);
+    if (g.tile_start) cudaFree(g.tile_start);
+  }
+  for (auto& dg : b->dtg)
+    if (dg.d) cudaFree(dg.d);
+  if (b->aux) cudaFree(b->aux);
+  for (fvm_handle* h : b->h) fvm_destroy(h);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return FVM_OK;
+}
+
+int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
+  if (!descs || !out || n < 1) return fail(FVM_E_INVALID, "fvm_batch_create: need n >= 1 descriptors");
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (descs[i].integrator != descs[0].integrator)
+      return fail(FVM_E_INVALID, "fvm_batch_create: all grids of a batch must use the same time integrator");
+    if (descs[i].precision != descs[0].precision)
+      return fail(FVM_E_INVALID, "fvm_batch_create: all grids of a batch must use the same precision");
+    if (descs[i].physics == FVM_MAXWELL)
+      return fail(FVM_E_INVALID, "fvm_batch_create: batches hold navier_stokes and heat grids");
+  }
+  fvm_batch* b = new fvm_batch();
+  b->integrator = descs[0].integrator;
+  b->f64 = descs[0].precision == FVM_FP64;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev);
+  auto bail = [&](int rc) { fvm_batch_destroy(b); return rc; };
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(FVM_E_CUDA, "stream creation failed"));
+  for (int i = 0; i < n; ++i) {
+    fvm_handle* h = nullptr;
+    const int rc = fvm_create(&descs[i], &h);
+    if (rc) return bail(rc);
+    b->h.push_back(h);
+  }
+  // group by kernel specialisation
+  for (int i = 0; i < n; ++i) {
+    const fvm_desc& d = descs[i];
+    const int lim = kernel_limiter(d);
+    const bool visc = d.physics == FVM_NAVIER_STOKES && d.params[1] != 0.0;
+    fvm_batch::Group* g = nullptr;
+    for (auto& x : b->groups)
+      if (x.physics == d.physics && x.lim == lim && x.riem == d.riemann && x.coords == d.coords && x.visc == visc) g = &x;
+    if (!g) {
+      b->groups.emplace_back();
+      g = &b->groups.back();
+      g->physics = d.physics; g->lim = lim; g->riem = d.riemann; g->coords = d.coords; g->visc = visc;
+    }
+    g->members.push_back(i);
+  }
+  for (auto& g : b->groups) {
+    const int rc = b->f64 ? build_group_arrays<double>(b, g) : build_group_arrays<float>(b, g);
+    if (rc) return bail(rc);
+  }
+  // auxiliary per-instance table and NS dt groups
+  std::vector<BatchAux> aux(n);
+  long long faces = 0;
+  for (int i = 0; i < n; ++i) {
+    fvm_handle* h = b->h[i];
+    BatchAux& a = aux[i];
+    a.lay = h->lay;
+    for (int k = 0; k < 3; ++k) a.U[k] = h->U[k];
+    a.clk = h->clk;
+    a.status = h->status;
+    a.bc = make_bc(h->d, h->nv);
+    a.nv = h->nv;
+    a.cmode = h->d.physics == FVM_NAVIER_STOKES ? 0 : 2;
+    a.max_inv_l2 = h->max_inv_l2;
+    a.const_rate = h->const_rate;
+    a.face_start = faces;
+    faces += bc_face_count(h->lay, h->nv);
+  }
+  b->faces = faces;
+  if (cudaMalloc(&b->aux, n * sizeof(BatchAux)) != cudaSuccess ||
+      cudaMemcpy(b->aux, aux.data(), n * sizeof(BatchAux), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(FVM_E_CUDA, "batch table upload failed"));
+  for (int c = 0; c < 3; ++c) {
+    std::vector<BatchDt> v;
+    for (int i = 0; i < n; ++i) {
+      fvm_handle* h = b->h[i];
+      if (h->d.physics != FVM_NAVIER_STOKES || h->d.coords != c) continue;
+      v.push_back(BatchDt{h->U[0], h->lay, h->md, h->d.params[0], h->d.params[1], h->clk, h->status});
+    }
+    if (v.empty()) continue;
+    fvm_batch::DtGroup dg;
+    dg.coords = c;
+    dg.n = (int)v.size();
+    if (cudaMalloc(&dg.d, v.size() * sizeof(BatchDt)) != cudaSuccess ||
+        cudaMemcpy(dg.d, v.data(), v.size() * sizeof(BatchDt), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(FVM_E_CUDA, "batch dt table upload failed"));
+    b->dtg.push_back(dg);
+  }
+  *out = b;
+  return FVM_OK;
+}
+
+int fvm_batch_size(const fvm_batch* b, int* n, long long* tiles) {
+  if (!b) return fail(FVM_E_INVALID, "null batch");
+  if (n) *n = (int)b->h.size();
+  if (tiles) {
+    long long t = 0;
+    for (auto& g : b->groups) t += g.ntiles;
+    *tiles = t;
+  }
+  return FVM_OK;
+}
+
+int fvm_batch_handle(fvm_batch* b, int i, fvm_handle** h) {
+  if (!b || !h || i < 0 || i >= (int)b->h.size()) return fail(FVM_E_INVALID, "fvm_batch_handle: bad index");
+  *h = b->h[i];
+  return FVM_OK;
+}
+
+int fvm_batch_step(fvm_batch* b, int n_steps, int dt_mode) {
+  if (!b) return fail(FVM_E_INVALID, "null batch");
+  if (dt_mode != 0 && dt_mode != 1) return fail(FVM_E_INVALID, "dt_mode must be 0 (CFL) or 1 (fixed)");
+  int rc = batch_graph(b, dt_mode);
+  if (rc) return rc;
+  for (int s = 0; s < n_steps; ++s) FVM_CK(cudaGraphLaunch(b->graph[dt_mode], b->stream));
+  FVM_CK(cudaStreamSynchronize(b->stream));
+  return FVM_OK;
+}
+
+int fvm_batch_time_steps(fvm_batch* b, int n_steps, int dt_mode, double* ms) {
+  if (!b || !ms) return fail(FVM_E_INVALID, "null argument");
+  if (dt_mode != 0 && dt_mode != 1) return fail(FVM_E_INVALID, "dt_mode must be 0 (CFL) or 1 (fixed)");
+  int rc = batch_graph(b, dt_mode);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  FVM_CK(cudaEventCreate(&e0));
+  FVM_CK(cudaEventCreate(&e1));
+  FVM_CK(cudaEventRecord(e0, b->stream));
+  for (int s = 0; s < n_steps; ++s) FVM_CK(cudaGraphLaunch(b->graph[dt_mode], b->stream));
+  FVM_CK(cudaEventRecord(e1, b->stream));
+  FVM_CK(cudaEventSynchronize(e1));
+  float t = 0.f;
+  FVM_CK(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t;
+  return FVM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner: z-march depth (planes per tile) chosen by timing candidate
+// values on the actual grid(s); the state is saved and restored around the
+// trials.  Tile rows, the 32-column warp-wide tile and the 4-byte lane width
+// of the coalesced 128-byte rows are fixed per kernel specialisation.
+namespace {
+
+std::vector<int> zchunk_candidates(int nz) {
+  std::vector<int> c;
+  for (int z : {8, 16, 32, 48, 64, 96, 128, 192, 256})
+    if (z < nz) c.push_back(z);
+  c.push_back(nz);
+  return c;
+}
+
+struct Saved {
+  std::vector<void*> buf;
+  std::vector<Clock> clk;
+};
+
+int save_states(const std::vector<fvm_handle*>& hs, Saved& s) {
+  for (fvm_handle* h : hs) {
+    void* p = nullptr;
+    const size_t bytes = (size_t)h->lay.var_stride * h->nv * h->esz;
+    FVM_CK(cudaMalloc(&p, bytes));
+    FVM_CK(cudaMemcpy(p, h->U[0], bytes, cudaMemcpyDeviceToDevice));
+    s.buf.push_back(p);
+    Clock c;
+    FVM_CK(cudaMemcpy(&c, h->clk, sizeof(Clock), cudaMemcpyDeviceToHost));
+    s.clk.push_back(c);
+  }
+  return FVM_OK;
+}
+
+int restore_states(const std::vector<fvm_handle*>& hs, Saved& s, bool release) {
+  for (size_t i = 0; i < hs.size(); ++i) {
+    fvm_handle* h = hs[i];
+    FVM_CK(cudaMemcpy(h->U[0], s.buf[i], (size_t)h->lay.var_stride * h->nv * h->esz, cudaMemcpyDeviceToDevice));
+    FVM_CK(cudaMemcpy(h->clk, &s.clk[i], sizeof(Clock), cudaMemcpyHostToDevice));
+    if (release) cudaFree(s.buf[i]);
+  }
+  return FVM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fvm_autotune(fvm_handle* h, int* best_zchunk, double* best_ms) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  Saved sv;
+  int rc = save_states({h}, sv);
+  if (rc) return rc;
+  int best = h->zchunk;
+  double bt = 1e30;
+  for (int z : zchunk_candidates(h->d.nx3)) {
+    h->zchunk = z;
+    for (auto& g : h->graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    double ms = 0.0;
+    if ((rc = fvm_time_steps(h, 1, 0, &ms))) break;  // warm-up (builds the graph)
+    if ((rc = fvm_time_steps(h, 3, 0, &ms))) break;
+    if (ms < bt) { bt = ms; best = z; }
+    if ((rc = restore_states({h}, sv, false))) break;
+  }
+  const int rr = restore_states({h}, sv, true);
+  h->zchunk = best;
+  for (auto& g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  if (rc) return rc;
+  if (rr) return rr;
+  if (best_zchunk) *best_zchunk = best;
+  if (best_ms) *best_ms = bt / 3.0;
+  return FVM_OK;
+}
+
+int fvm_batch_autotune(fvm_batch* b, int* best_zchunk, double* best_ms) {
+  if (!b) return fail(FVM_E_INVALID, "null batch");
+  for (fvm_handle* h : b->h) FVM_CK(cudaStreamSynchronize(h->stream));
+  int nzmax = 1;
+  for (fvm_handle* h : b->h) nzmax = std::max(nzmax, h->d.nx3);
+  Saved sv;
+  int rc = save_states(b->h, sv);
+  if (rc) return rc;
+  int best = b->h[0]->zchunk;
+  double bt = 1e30;
+  auto apply = [&](int z) -> int {
+    for (fvm_handle* h : b->h) h->zchunk = z;
+    batch_drop_graphs(b);
+    for (auto& g : b->groups) {
+      const int r = b->f64 ? build_group_arrays<double>(b, g) : build_group_arrays<float>(b, g);
+      if (r) return r;
+    }
+    return FVM_OK;
+  };
+  for (int z : zchunk_candidates(nzmax)) {
+    if ((rc = apply(z))) break;
+    double ms = 0.0;
+    if ((rc = fvm_batch_time_steps(b, 1, 0, &ms))) break;
+    if ((rc = fvm_batch_time_steps(b, 3, 0, &ms))) break;
+    if (ms < bt) { bt = ms; best = z; }
+    if ((rc = restore_states(b->h, sv, false))) break;
+  }
+  const int rr = restore_states(b->h, sv, true);
+  const int ra = apply(best);
+  if (rc) return rc;
+  if (rr) return rr;
+  if (ra) return ra;
+  if (best_zchunk) *best_zchunk = best;
+  if (best_ms) *best_ms = bt / 3.0;
+  return FVM_OK;
+}
+
+}  // extern "C"

@@ -12,14 +12,16 @@ struct BcSpec {
 // Ghost face slabs of every variable (boundary_conditions.py:13-91 applied
 // per variable and side as in solver.py:30-37).  Edges and corners are never
 // read by the residual, so only the six face slabs are filled here.
+__host__ __device__ inline long long bc_face_count(const Layout& L, int nv) {
+  return 2ll * nv * ((long long)L.ny * L.nz + (long long)L.nx * L.nz + (long long)L.nx * L.ny);
+}
+
+// Fill ghost element t (0 <= t < bc_face_count) of one grid.
 template <typename Real>
-__global__ void bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc, const int* active) {
-  if (active && !*active) return;
+__device__ __forceinline__ void bc_fill_one(Real* __restrict__ u, const Layout& L, const BcSpec& bc, long long t) {
   const long long nyz = (long long)L.ny * L.nz, nxz = (long long)L.nx * L.nz, nxy = (long long)L.nx * L.ny;
   const long long per_var = 2 * (nyz + nxz + nxy);
-  const long long total = per_var * nv;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
+  {
     const int q = (int)(t / per_var);
     long long r = t % per_var;
     int side, a, b;  // a, b: transverse interior indices (0-based)
@@ -43,6 +45,15 @@ __global__ void bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc
     else out = v;
     u[gi] = out;
   }
+}
+
+template <typename Real>
+__global__ void bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc, const int* active) {
+  if (active && !*active) return;
+  const long long total = bc_face_count(L, nv);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    bc_fill_one(u, L, bc, t);
 }
 
 // Reference layout (C order, last axis fastest) <-> device layout (x1 fastest).
@@ -87,6 +98,34 @@ struct Clock {
   unsigned long long red[2];  // running maxima (bit patterns of non-negative doubles)
 };
 
+// ------------------------------------------------------------- batches ----
+// Per-instance data of the batched auxiliary kernels.
+struct BatchAux {
+  Layout lay;
+  void* U[3];
+  Clock* clk;
+  unsigned* status;
+  BcSpec bc;
+  int nv, cmode;  // clock mode (0 NS rates, 1 fixed, 2 constant)
+  double max_inv_l2, const_rate;
+  long long face_start;  // prefix sum of ghost elements
+};
+
+template <typename Real>
+__global__ void batch_bc_kernel(const BatchAux* __restrict__ a, int n, long long total, int buf) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a[mid].face_start <= t) lo = mid; else hi = mid - 1;
+    }
+    const BatchAux& x = a[lo];
+    if (!x.clk->active) continue;
+    bc_fill_one(static_cast<Real*>(x.U[buf]), x.lay, x.bc, t - x.face_start);
+  }
+}
+
 __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
   atomicMax(a, (unsigned long long)__double_as_longlong(v));
 }
@@ -94,8 +133,33 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) 
 // CFL rates of the Navier-Stokes state (navier_stokes.py:512-585) in float64:
 // red[0] = max_cells max_d max_w |v_d + kappa_w| / L_d, red[1] = max mu/rho.
 template <typename Real, int COORD>
+__device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, const Layout& L, const Metric<double>& m,
+                                                  double gam, double mu, Clock* clk, unsigned* status);
+
+template <typename Real, int COORD>
 __global__ void ns_dt_reduce_kernel(const Real* __restrict__ u, Layout L, Metric<double> m, double gam, double mu,
                                     Clock* clk, unsigned* status) {
+  ns_dt_reduce_body<Real, COORD>(u, L, m, gam, mu, clk, status);
+}
+
+// Per-instance CFL rates of a batch of Navier-Stokes grids: blockIdx.y picks the grid.
+struct BatchDt {
+  const void* u;
+  Layout lay;
+  Metric<double> md;
+  double gam, mu;
+  Clock* clk;
+  unsigned* status;
+};
+template <typename Real, int COORD>
+__global__ void batch_ns_dt_kernel(const BatchDt* __restrict__ b) {
+  const BatchDt& x = b[blockIdx.y];
+  ns_dt_reduce_body<Real, COORD>(static_cast<const Real*>(x.u), x.lay, x.md, x.gam, x.mu, x.clk, x.status);
+}
+
+template <typename Real, int COORD>
+__device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, const Layout& L, const Metric<double>& m,
+                                                  double gam, double mu, Clock* clk, unsigned* status) {
   if (!clk->active) return;
   __shared__ double s_rc[32], s_nu[32];
   double rc = 0.0, nu = 0.0;
@@ -150,7 +214,8 @@ __global__ void ns_dt_reduce_kernel(const Real* __restrict__ u, Layout L, Metric
 // One thread: close the step's clock.  mode 0: dt from the reduced NS rates,
 // mode 1: fixed dt, mode 2: dt = cfl / const_rate (state-independent heat and
 // Maxwell steps).  `max_inv_l2` = max over cells of sum_d 1/L_d^2.
-__global__ void clock_kernel(Clock* clk, int mode, double max_inv_l2, double const_rate, unsigned* status) {
+__device__ __forceinline__ void clock_one(Clock* clk, int mode, double max_inv_l2, double const_rate,
+                                          unsigned* status) {
   clk->active = clk->t <= clk->t_end ? 1 : 0;
   double dt;
   if (mode == 0) {
@@ -170,6 +235,15 @@ __global__ void clock_kernel(Clock* clk, int mode, double max_inv_l2, double con
   clk->dt = dt;
   clk->t = clk->t + dt;
   clk->steps = clk->steps + 1;
+}
+
+__global__ void clock_kernel(Clock* clk, int mode, double max_inv_l2, double const_rate, unsigned* status) {
+  clock_one(clk, mode, max_inv_l2, const_rate, status);
+}
+
+__global__ void batch_clock_kernel(const BatchAux* __restrict__ a, int n, int fixed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) clock_one(a[i].clk, fixed ? 1 : a[i].cmode, a[i].max_inv_l2, a[i].const_rate, a[i].status);
 }
 
 // Conserved totals with Neumaier compensation: per-thread, then per-block

@@ -316,7 +316,36 @@ __device__ __forceinline__ R stage_combine(const StageCoef& c, R dt, R k, R ucur
       // coefficients 1/3, 2/3 do not sum to one and would bias the totals)
       if constexpr (sizeof(R) == 4) return u0 + R(c.cb) * ((ucur - u0) + dt * k);
       else return R(c.ca) * u0 + R(c.cb) * (ucur + dt * k);
-    default: return u0 + (dt / R(6)) * (acc + k);
+    default:
+      // float32 keeps acc = U0 + (dt/6) sum_s w_s k_s (low storage: the last
+      // stage reads only its input and acc); float64 keeps the k-sum and the
+      // reference's summation order U0 + (dt/6)(k1 + w k2 + ... + k_last)
+      if constexpr (sizeof(R) == 4) return acc + (dt / R(6)) * k;
+      else return u0 + (dt / R(6)) * (acc + k);
+  }
+}
+
+// The stage epilogue needs U0 from memory (not from the input ring)?
+template <typename R>
+__device__ __forceinline__ bool needs_u0(const StageCoef& c) {
+  if (c.mode < MODE_AXPY) return false;
+  if constexpr (sizeof(R) == 4) {
+    if (c.mode == MODE_FINAL) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ bool needs_acc(const StageCoef& c) {
+  return c.mode == MODE_FINAL || c.accmode == ACC_ADD;
+}
+// New accumulator value after this stage (see stage_combine).
+template <typename R>
+__device__ __forceinline__ R acc_update(const StageCoef& c, R dt, R k, R u0, R acc) {
+  if constexpr (sizeof(R) == 4) {
+    if (c.accmode == ACC_SET) return u0 + (dt / R(6)) * k;
+    return acc + ((R(c.wacc) * dt) / R(6)) * k;
+  } else {
+    if (c.accmode == ACC_SET) return k;
+    return acc + R(c.wacc) * k;
   }
 }
 

@@ -3,4 +3,6 @@
 namespace fvm {
 template cudaError_t launch_ns_coord<double, COORD_CYL>(int, int, bool, const CUtensorMap&, const NsParams<double>&,
                                                      cudaStream_t, int);
+template cudaError_t launch_ns_batch_coord<double, COORD_CYL>(int, int, bool, const BatchSource<NsParams<double>>&, long long,
+                                                           cudaStream_t, int);
 }

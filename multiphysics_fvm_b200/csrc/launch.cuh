@@ -28,24 +28,38 @@ static cudaError_t prepare_kernel(K kern, int threads, int bytes, int* blocks_pe
 
 // nsm < 0: only set the kernel's shared-memory attribute and query its
 // occupancy (done once, outside any stream capture).
-template <typename Real, int LIM, int RIEM, int COORD, bool VISC>
-cudaError_t launch_ns_one(const CUtensorMap& map, NsParams<Real> p, cudaStream_t s, int nsm) {
+template <typename Real, int LIM, int RIEM, int COORD, bool VISC, class Src>
+cudaError_t launch_ns_src(const Src& src, long long ntiles, cudaStream_t s, int nsm) {
   constexpr int TY = ns_tile_ty<Real, VISC>();
   using C = NsCfg<Real, VISC, TY>;
-  auto kern = ns_stage_kernel<Real, LIM, RIEM, COORD, VISC, TY, ns_min_blocks<Real, VISC>()>;
+  auto kern = ns_stage_kernel<Real, LIM, RIEM, COORD, VISC, TY, ns_min_blocks<Real, VISC>(), Src>;
   static int bps = 0;
   if (bps == 0 || nsm < 0) {
     cudaError_t e = prepare_kernel(kern, C::NT, C::BYTES, &bps);
     if (e != cudaSuccess) return e;
   }
   if (nsm < 0) return cudaSuccess;
-  p.ntx = (p.lay.nx + C::TX - 1) / C::TX;
-  p.nty = (p.lay.ny + TY - 1) / TY;
-  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
-  const long long ntiles = (long long)p.ntx * p.nty * p.nzc;
+  if (ntiles <= 0) return cudaSuccess;
   const int grid = (int)(ntiles < (long long)bps * nsm ? ntiles : (long long)bps * nsm);
-  kern<<<grid, C::NT, C::BYTES, s>>>(map, p);
+  kern<<<grid, C::NT, C::BYTES, s>>>(src);
   return cudaGetLastError();
+}
+
+template <typename Real, bool VISC>
+void ns_tile_counts(NsParams<Real>& p) {
+  constexpr int TY = ns_tile_ty<Real, VISC>();
+  p.ntx = (p.lay.nx + 31) / 32;
+  p.nty = (p.lay.ny + TY - 1) / TY;
+  p.nzc = p.flat ? 1 : (p.lay.nz + p.zchunk - 1) / p.zchunk;
+}
+
+template <typename Real, int LIM, int RIEM, int COORD, bool VISC>
+cudaError_t launch_ns_one(const CUtensorMap& map, NsParams<Real> p, cudaStream_t s, int nsm) {
+  ns_tile_counts<Real, VISC>(p);
+  SingleSource<NsParams<Real>> src;
+  src.tmap = map;
+  src.p = p;
+  return launch_ns_src<Real, LIM, RIEM, COORD, VISC>(src, (long long)p.ntx * p.nty * p.nzc, s, nsm);
 }
 
 template <typename Real, int COORD>
@@ -67,16 +81,47 @@ cudaError_t launch_ns_coord(int lim, int riem, bool visc, const CUtensorMap& map
   return cudaErrorInvalidValue;
 }
 
+// Batched launch: every instance shares the kernel specialisation; the tile
+// counts of each instance's params must already be filled in.
+template <typename Real, int COORD>
+cudaError_t launch_ns_batch_coord(int lim, int riem, bool visc, const BatchSource<NsParams<Real>>& src,
+                                  long long ntiles, cudaStream_t s, int nsm) {
+#define FVM_NS_CASE(L, R)                                                                                \
+  if (lim == L && riem == R)                                                                             \
+    return visc ? launch_ns_src<Real, L, R, COORD, true>(src, ntiles, s, nsm)                            \
+                : launch_ns_src<Real, L, R, COORD, false>(src, ntiles, s, nsm);
+  FVM_NS_CASE(LIM_PC, RIEM_RUSANOV)
+  FVM_NS_CASE(LIM_PC, RIEM_HLL)
+  FVM_NS_CASE(LIM_MINMOD, RIEM_RUSANOV)
+  FVM_NS_CASE(LIM_MINMOD, RIEM_HLL)
+  FVM_NS_CASE(LIM_MC, RIEM_RUSANOV)
+  FVM_NS_CASE(LIM_MC, RIEM_HLL)
+  FVM_NS_CASE(LIM_VANLEER, RIEM_RUSANOV)
+  FVM_NS_CASE(LIM_VANLEER, RIEM_HLL)
+#undef FVM_NS_CASE
+  return cudaErrorInvalidValue;
+}
+
 // Declarations of the per-(precision, coordinate) instantiations.
 #define FVM_DECLARE_NS(REAL, COORD)                                                                      \
   extern template cudaError_t launch_ns_coord<REAL, COORD>(int, int, bool, const CUtensorMap&,          \
-                                                          const NsParams<REAL>&, cudaStream_t, int);
+                                                          const NsParams<REAL>&, cudaStream_t, int);    \
+  extern template cudaError_t launch_ns_batch_coord<REAL, COORD>(                                        \
+      int, int, bool, const BatchSource<NsParams<REAL>>&, long long, cudaStream_t, int);
 FVM_DECLARE_NS(float, COORD_CART)
 FVM_DECLARE_NS(float, COORD_CYL)
 FVM_DECLARE_NS(float, COORD_SPH)
 FVM_DECLARE_NS(double, COORD_CART)
 FVM_DECLARE_NS(double, COORD_CYL)
 FVM_DECLARE_NS(double, COORD_SPH)
+
+template <typename Real>
+cudaError_t launch_ns_batch(int lim, int riem, int coord, bool visc, const BatchSource<NsParams<Real>>& src,
+                            long long ntiles, cudaStream_t s, int nsm) {
+  if (coord == COORD_CART) return launch_ns_batch_coord<Real, COORD_CART>(lim, riem, visc, src, ntiles, s, nsm);
+  if (coord == COORD_CYL) return launch_ns_batch_coord<Real, COORD_CYL>(lim, riem, visc, src, ntiles, s, nsm);
+  return launch_ns_batch_coord<Real, COORD_SPH>(lim, riem, visc, src, ntiles, s, nsm);
+}
 
 template <typename Real>
 cudaError_t launch_ns(int lim, int riem, int coord, bool visc, const CUtensorMap& map, const NsParams<Real>& p,
@@ -87,34 +132,36 @@ cudaError_t launch_ns(int lim, int riem, int coord, bool visc, const CUtensorMap
 }
 
 // ---------------------------------------------------------------- heat ----
-template <typename Real, int LIM, int COORD>
-cudaError_t launch_heat_one(const CUtensorMap& map, HeatParams<Real> p, cudaStream_t s, int nsm) {
+template <typename Real, int LIM, int COORD, class Src>
+cudaError_t launch_heat_src(const Src& src, long long ntiles, cudaStream_t s, int nsm) {
   constexpr int TY = 8;
   using C = HeatCfg<Real, LIM, TY>;
-  auto kern = heat_stage_kernel<Real, LIM, COORD, TY>;
+  auto kern = heat_stage_kernel<Real, LIM, COORD, TY, Src>;
   static int bps = 0;
   if (bps == 0 || nsm < 0) {
     cudaError_t e = prepare_kernel(kern, C::NT, C::BYTES, &bps);
     if (e != cudaSuccess) return e;
   }
-  if (nsm < 0) return cudaSuccess;
-  p.ntx = (p.lay.nx + C::TX - 1) / C::TX;
-  p.nty = (p.lay.ny + TY - 1) / TY;
-  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
-  const long long ntiles = (long long)p.ntx * p.nty * p.nzc;
+  if (nsm < 0 || ntiles <= 0) return cudaSuccess;
   const int grid = (int)(ntiles < (long long)bps * nsm ? ntiles : (long long)bps * nsm);
-  kern<<<grid, C::NT, C::BYTES, s>>>(map, p);
+  kern<<<grid, C::NT, C::BYTES, s>>>(src);
   return cudaGetLastError();
 }
 
 template <typename Real>
-cudaError_t launch_heat(int lim, int coord, const CUtensorMap& map, const HeatParams<Real>& p, cudaStream_t s,
-                        int nsm) {
-#define FVM_HEAT_CASE(L)                                                                       \
-  if (lim == L) {                                                                              \
-    if (coord == COORD_CART) return launch_heat_one<Real, L, COORD_CART>(map, p, s, nsm);     \
-    if (coord == COORD_CYL) return launch_heat_one<Real, L, COORD_CYL>(map, p, s, nsm);       \
-    return launch_heat_one<Real, L, COORD_SPH>(map, p, s, nsm);                               \
+void heat_tile_counts(HeatParams<Real>& p) {
+  p.ntx = (p.lay.nx + 31) / 32;
+  p.nty = (p.lay.ny + 7) / 8;
+  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
+}
+
+template <typename Real, class Src>
+cudaError_t launch_heat_any(int lim, int coord, const Src& src, long long ntiles, cudaStream_t s, int nsm) {
+#define FVM_HEAT_CASE(L)                                                                               \
+  if (lim == L) {                                                                                      \
+    if (coord == COORD_CART) return launch_heat_src<Real, L, COORD_CART>(src, ntiles, s, nsm);         \
+    if (coord == COORD_CYL) return launch_heat_src<Real, L, COORD_CYL>(src, ntiles, s, nsm);           \
+    return launch_heat_src<Real, L, COORD_SPH>(src, ntiles, s, nsm);                                   \
   }
   FVM_HEAT_CASE(LIM_PC)
   FVM_HEAT_CASE(LIM_MINMOD)
@@ -123,8 +170,28 @@ cudaError_t launch_heat(int lim, int coord, const CUtensorMap& map, const HeatPa
 #undef FVM_HEAT_CASE
   return cudaErrorInvalidValue;
 }
+
+template <typename Real>
+cudaError_t launch_heat(int lim, int coord, const CUtensorMap& map, const HeatParams<Real>& p0, cudaStream_t s,
+                        int nsm) {
+  HeatParams<Real> p = p0;
+  heat_tile_counts(p);
+  SingleSource<HeatParams<Real>> src;
+  src.tmap = map;
+  src.p = p;
+  return launch_heat_any<Real>(lim, coord, src, (long long)p.ntx * p.nty * p.nzc, s, nsm);
+}
+template <typename Real>
+cudaError_t launch_heat_batch(int lim, int coord, const BatchSource<HeatParams<Real>>& src, long long ntiles,
+                              cudaStream_t s, int nsm) {
+  return launch_heat_any<Real>(lim, coord, src, ntiles, s, nsm);
+}
 extern template cudaError_t launch_heat<float>(int, int, const CUtensorMap&, const HeatParams<float>&, cudaStream_t, int);
 extern template cudaError_t launch_heat<double>(int, int, const CUtensorMap&, const HeatParams<double>&, cudaStream_t, int);
+extern template cudaError_t launch_heat_batch<float>(int, int, const BatchSource<HeatParams<float>>&, long long,
+                                                     cudaStream_t, int);
+extern template cudaError_t launch_heat_batch<double>(int, int, const BatchSource<HeatParams<double>>&, long long,
+                                                      cudaStream_t, int);
 
 // ------------------------------------------------------------- maxwell ----
 // Maxwell: 6 rows x 32 columns, 2 blocks of 256 threads per SM (float32).

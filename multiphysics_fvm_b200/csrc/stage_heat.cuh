@@ -51,9 +51,9 @@ struct HeatCfg {
   static constexpr unsigned TX_BYTES = PL * sizeof(Real);
 };
 
-template <typename Real, int LIM, int COORD, int TY>
+template <typename Real, int LIM, int COORD, int TY, class Src>
 __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
-    heat_stage_kernel(const __grid_constant__ CUtensorMap tmap, const HeatParams<Real> p) {
+    heat_stage_kernel(const __grid_constant__ Src src) {
   using C = HeatCfg<Real, LIM, TY>;
   using G = Geo<Real, COORD>;
   constexpr int TX = C::TX, NT = C::NT, W = C::W, PL = C::PL, HH = C::HH;
@@ -66,19 +66,13 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
   Real* fR = sm + C::OFF_FR;
   Real* fb = sm + C::OFF_FB;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (C::BYTES - C::NSLOT * 8));
-  if (p.active && !*p.active) return;
   if (smem_u32(smem_raw) & 127u) {
-    if (threadIdx.x == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+    if (threadIdx.x == 0) atomicOr(src.params(0).status, ST_TMA_TIMEOUT);
     return;
   }
   const int tid = threadIdx.x;
-  const Layout& L = p.lay;
-  const int nx = L.nx, ny = L.ny, nz = L.nz;
-  const Real rcp = Real(p.rho_cp), kk = Real(p.k), qsrc = Real(p.q), ircp = Real(p.inv_rho_cp);
   constexpr bool F32 = sizeof(Real) == 4;
-  const Real dt = Real(*p.dt);
   if (tid == 0) {
-    tma_prefetch_desc(&tmap);
     for (int s = 0; s < C::NSLOT; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
   }
@@ -90,9 +84,19 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
 
   const bool is_out = tid < TX * TY;
   const int otx = tid % TX, oty = tid / TX;
-  const int ntiles = p.ntx * p.nty * p.nzc;
+  const int ntiles = src.total();
   bool ok = true;
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+  for (int gtile = blockIdx.x; gtile < ntiles && ok; gtile += gridDim.x) {
+    const int inst = src.instance(gtile);
+    const HeatParams<Real>& p = src.params(inst);
+    if (p.active && !*p.active) continue;  // this grid's clock passed t_end
+    const CUtensorMap* tmap = src.map(inst);
+    const int tile = src.local(gtile, inst);
+    const Layout& L = p.lay;
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const Real rcp = Real(p.rho_cp), kk = Real(p.k), qsrc = Real(p.q), ircp = Real(p.inv_rho_cp);
+    const Real dt = Real(*p.dt);
+    if (tid == 0) tma_prefetch_desc(tmap);
     const int x0 = (tile % p.ntx) * TX, y0 = ((tile / p.ntx) % p.nty) * TY;
     const int Z0 = 1 + (tile / (p.ntx * p.nty)) * p.zchunk;
     const int Zl = min(Z0 + p.zchunk - 1, nz);
@@ -106,7 +110,7 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
       pending |= 1u << s;
       fence_proxy_async();
       mbar_arrive_expect_tx(&bars[s], C::TX_BYTES);
-      tma_load_4d(&uring[s * C::SLOT], &tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
+      tma_load_4d(&uring[s * C::SLOT], tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
     };
     if (tid == 0) issue(Pfirst);
     for (int K = Kfirst; K <= Zl; ++K) {
@@ -206,12 +210,11 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
           const long long gi = L.idx(0, K, oj + 1, oi + 1);
           const Real ucur = U(K, oty + HH, otx + 4);
           Real u0v = Real(0), accv = Real(0);
-          if (p.coef.mode >= MODE_AXPY) u0v = p.coef.u0_is_input ? ucur : p.u0[gi];
-          if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
+          if (needs_u0<Real>(p.coef)) u0v = p.coef.u0_is_input ? ucur : p.u0[gi];
+          if (needs_acc(p.coef)) accv = p.acc[gi];
           const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
           p.out[gi] = o;
-          if (p.coef.accmode == ACC_SET) p.acc[gi] = k;
-          else if (p.coef.accmode == ACC_ADD) p.acc[gi] = accv + Real(p.coef.wacc) * k;
+          if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
           if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
         }
         __syncthreads();
@@ -219,8 +222,8 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
       }
       if (out_valid && otx == 0) {
         const long long g0 = L.idx(0, K, oj + 1, oi + 1);
-        if (p.coef.mode >= MODE_AXPY && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0);
-        if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) prefetch_l2(p.acc + g0);
+        if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0);
+        if (needs_acc(p.coef)) prefetch_l2(p.acc + g0);
       }
       // x1 faces of plane K
       for (int it = tid; it < TY * (TX + 2); it += NT) {
@@ -281,12 +284,11 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         const long long gi = L.idx(0, K, oj + 1, oi + 1);
         const Real ucur = U(K, oty + HH, otx + 4);
         Real u0v = Real(0), accv = Real(0);
-        if (p.coef.mode >= MODE_AXPY) u0v = p.coef.u0_is_input ? ucur : p.u0[gi];
-        if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
+        if (needs_u0<Real>(p.coef)) u0v = p.coef.u0_is_input ? ucur : p.u0[gi];
+        if (needs_acc(p.coef)) accv = p.acc[gi];
         const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
         p.out[gi] = o;
-        if (p.coef.accmode == ACC_SET) p.acc[gi] = k;
-        else if (p.coef.accmode == ACC_ADD) p.acc[gi] = accv + Real(p.coef.wacc) * k;
+        if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
         if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
       }
       __syncthreads();

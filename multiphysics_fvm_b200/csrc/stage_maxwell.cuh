@@ -250,8 +250,8 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
       if (out_valid && otx == 0) {
         const long long g0 = L.idx(0, K, oj + 1, oi + 1);
         for (int v = 0; v < NV; ++v) {
-          if (p.coef.mode >= MODE_AXPY && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
-          if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) prefetch_l2(p.acc + g0 + v * L.var_stride);
+          if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
+          if (needs_acc(p.coef)) prefetch_l2(p.acc + g0 + v * L.var_stride);
         }
       }
       // x1 faces
@@ -403,12 +403,11 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
           else k = (-sum) / Vc + ((sg[v] + sp) + sc[v]);
           const long long gi = gidx + (long long)v * L.var_stride;
           Real u0v = Real(0), accv = Real(0);
-          if (p.coef.mode >= MODE_AXPY) u0v = p.coef.u0_is_input ? q[v] : p.u0[gi];
-          if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
+          if (needs_u0<Real>(p.coef)) u0v = p.coef.u0_is_input ? q[v] : p.u0[gi];
+          if (needs_acc(p.coef)) accv = p.acc[gi];
           const Real o = stage_combine(p.coef, dt, k, q[v], u0v, accv);
           p.out[gi] = o;
-          if (p.coef.accmode == ACC_SET) p.acc[gi] = k;
-          else if (p.coef.accmode == ACC_ADD) p.acc[gi] = accv + Real(p.coef.wacc) * k;
+          if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
           if (!isfinite(o)) bad |= ST_NONFINITE;
         }
         if (bad) atomicOr(p.status, bad);

@@ -31,6 +31,40 @@ struct NsParams {
   double gamma, mu, g1, g2, g3;
   unsigned* status;
   int zchunk, ntx, nty, nzc;
+  int flat;  // nx3 == 1 with x3 ghosts equal to the plane: x3 fluxes cancel, no z-march
+};
+
+// Tile sources: one grid (params + tensor map in kernel parameter space) or a
+// batch of independent grids (per-instance params and maps in global memory,
+// one flat tile list, instance found by binary search over tile offsets).
+template <class P>
+struct SingleSource {
+  CUtensorMap tmap;
+  P p;
+  __device__ __forceinline__ int total() const { return p.ntx * p.nty * p.nzc; }
+  __device__ __forceinline__ int instance(int) const { return 0; }
+  __device__ __forceinline__ const P& params(int) const { return p; }
+  __device__ __forceinline__ const CUtensorMap* map(int) const { return &tmap; }
+  __device__ __forceinline__ int local(int g, int) const { return g; }
+};
+template <class P>
+struct BatchSource {
+  const P* prm;             // per instance (this stage)
+  const CUtensorMap* maps;  // per instance: map of this stage's input buffer
+  const int* tile_start;    // ninst+1 prefix sums of tiles
+  int ninst;
+  __device__ __forceinline__ int total() const { return __ldg(tile_start + ninst); }
+  __device__ __forceinline__ int instance(int g) const {
+    int lo = 0, hi = ninst - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(tile_start + mid) <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ const P& params(int i) const { return prm[i]; }
+  __device__ __forceinline__ const CUtensorMap* map(int i) const { return maps + i; }
+  __device__ __forceinline__ int local(int g, int i) const { return g - __ldg(tile_start + i); }
 };
 
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
@@ -129,9 +163,9 @@ __device__ __forceinline__ void ns_flux(const R* qL, const R* qR, R gam, R F[5])
   }
 }
 
-template <typename Real, int LIM, int RIEM, int COORD, bool VISC, int TY, int MINB>
+template <typename Real, int LIM, int RIEM, int COORD, bool VISC, int TY, int MINB, class Src>
 __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
-    ns_stage_kernel(const __grid_constant__ CUtensorMap tmap, const NsParams<Real> p) {
+    ns_stage_kernel(const __grid_constant__ Src src) {
   using C = NsCfg<Real, VISC, TY>;
   using G = Geo<Real, COORD>;
   constexpr int TX = C::TX, NT = C::NT, W = C::W, PL = C::PL, HH = C::HH, NREC = C::NREC;
@@ -147,19 +181,12 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
   Real* fb = sm + C::OFF_FB;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (C::BYTES - C::NSLOT * 8));
 
-  if (p.active && !*p.active) return;
   if (smem_u32(smem_raw) & 127u) {  // TMA destinations need 128-byte alignment
-    if (threadIdx.x == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+    if (threadIdx.x == 0) atomicOr(src.params(0).status, ST_TMA_TIMEOUT);
     return;
   }
   const int tid = threadIdx.x;
-  const Layout& L = p.lay;
-  const int nx = L.nx, ny = L.ny, nz = L.nz;
-  const Real gam = Real(p.gamma), mu = Real(p.mu);
-  const Real dt = Real(*p.dt);
-
   if (tid == 0) {
-    tma_prefetch_desc(&tmap);
     for (int s = 0; s < C::NSLOT; ++s) mbar_init(&bars[s], 1);
     mbar_fence_init();
   }
@@ -179,17 +206,29 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
   const bool is_out = tid < TX * TY;
   const int otx = tid % TX, oty = tid / TX;
 
-  const int ntiles = p.ntx * p.nty * p.nzc;
+  const int ntiles = src.total();
   bool ok = true;
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+  for (int gtile = blockIdx.x; gtile < ntiles && ok; gtile += gridDim.x) {
+    const int inst = src.instance(gtile);
+    const NsParams<Real>& p = src.params(inst);
+    if (p.active && !*p.active) continue;  // this grid's clock passed t_end
+    const CUtensorMap* tmap = src.map(inst);
+    const int tile = src.local(gtile, inst);
+    const Layout& L = p.lay;
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const Real gam = Real(p.gamma), mu = Real(p.mu);
+    const Real dt = Real(*p.dt);
+    const bool flat = p.flat != 0;
+    if (tid == 0) tma_prefetch_desc(tmap);
     const int tx_i = tile % p.ntx;
     const int ty_i = (tile / p.ntx) % p.nty;
     const int zc_i = tile / (p.ntx * p.nty);
     const int x0 = tx_i * TX, y0 = ty_i * TY;
     const int Z0 = 1 + zc_i * p.zchunk;         // first ghosted output plane
     const int Zl = min(Z0 + p.zchunk - 1, nz);  // last ghosted output plane
-    const int Pfirst = Z0 - HH, Plast = Zl + HH;
-    const int Kfirst = Z0 - 4;  // first step: P (and tau) of plane Z0-2
+    // flat grids: only plane 1, no x3 pipeline
+    const int Pfirst = flat ? Z0 : Z0 - HH, Plast = flat ? Zl : Zl + HH;
+    const int Kfirst = flat ? Z0 : Z0 - 4;  // first step: P (and tau) of plane Z0-2
 
     const int oi = x0 + otx, oj = y0 + oty;  // output cell (interior 0-based)
     const bool out_valid = is_out && oi < nx && oj < ny;
@@ -206,7 +245,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       pending |= 1u << s;
       fence_proxy_async();
       mbar_arrive_expect_tx(&bars[s], C::TX_BYTES);
-      tma_load_4d(&uring[s * C::SLOT], &tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
+      tma_load_4d(&uring[s * C::SLOT], tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
     };
     // planes needed by the first step plus one of prefetch
     if (tid == 0)
@@ -217,7 +256,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       if (tid == 0 && K > Kfirst && K + HH + 1 <= Plast) issue(K + HH + 1);
       {
         bool got = true;
-        for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= K + HH; ++pl) {
+        const int wlast = flat ? K : K + HH;
+        for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= wlast; ++pl) {
           const int s = pmod(pl, C::NSLOT);
           got = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 2000000000ull);
           phase_bits ^= (1u << s);
@@ -228,7 +268,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
           break;
         }
         if (tid == 0)
-          for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= K + HH; ++pl) pending &= ~(1u << pmod(pl, C::NSLOT));
+          for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= wlast; ++pl) pending &= ~(1u << pmod(pl, C::NSLOT));
       }
       const int sK = pmod(K, C::NSLOT), sK1 = pmod(K + 1, C::NSLOT), sK2 = pmod(K + 2, C::NSLOT);
       // ring bases of planes K, K+1, K+2 (uniform, once per step)
@@ -245,8 +285,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       if (K >= Z0 && out_valid && otx == 0) {
         const long long g0 = L.idx(0, K, oj + 1, oi + 1);
         for (int v = 0; v < 5; ++v) {
-          if (p.coef.mode >= MODE_AXPY && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
-          if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) prefetch_l2(p.acc + g0 + v * L.var_stride);
+          if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
+          if (needs_acc(p.coef)) prefetch_l2(p.acc + g0 + v * L.var_stride);
         }
       }
       // ---------------------------------------------------------- B ----
@@ -275,10 +315,11 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       // ---------------------------------------------------------- C ----
       // P on plane K+2, tile + 2 (navier_stokes.py:94-100)
       {
-        Real* pw = pring + pmod(K + 2, 3) * PL2;
+        Real* pw = pring + pmod(flat ? K : K + 2, 3) * PL2;
+        const Real* usrc = flat ? uK : uK2;
         for (int it = tid; it < C::PL2; it += NT) {
           const int r2 = it / W2, c2 = it % W2;
-          const Real* u = uK2 + (r2 + HH - 2) * W + c2 + 2;
+          const Real* u = usrc + (r2 + HH - 2) * W + c2 + 2;
           const Real rho = u[0];
           Real v0, v1, v2, E;
           if constexpr (F32) {
@@ -367,7 +408,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       // -------------------------------------------------------- E, F ----
       // x3 slopes of cell K+1 and the x3 face flux at K+1/2 (registers);
       // tau row 3 = (t13, t23, t33)
-      if (K >= Z0 - 2 && is_out) {
+      if (!flat && K >= Z0 - 2 && is_out) {
         constexpr int ti[3] = {4, 5, 2};
         const int kk = K;  // interior index of plane K+1
         const bool ghost = (K + 1 <= 0 || K + 1 >= nz + 1);
@@ -563,12 +604,11 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
           else k = (-sum) / Vc + src[v];
           const long long gi = gidx + (long long)v * L.var_stride;
           Real u0v = Real(0), accv = Real(0);
-          if (p.coef.mode >= MODE_AXPY) u0v = p.coef.u0_is_input ? q[v] : p.u0[gi];
-          if (p.coef.mode == MODE_FINAL || p.coef.accmode == ACC_ADD) accv = p.acc[gi];
+          if (needs_u0<Real>(p.coef)) u0v = p.coef.u0_is_input ? q[v] : p.u0[gi];
+          if (needs_acc(p.coef)) accv = p.acc[gi];
           const Real o = stage_combine(p.coef, dt, k, q[v], u0v, accv);
           p.out[gi] = o;
-          if (p.coef.accmode == ACC_SET) p.acc[gi] = k;
-          else if (p.coef.accmode == ACC_ADD) p.acc[gi] = accv + Real(p.coef.wacc) * k;
+          if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
           if (!isfinite(o)) bad |= ST_NONFINITE;
           if (v == 0 && p.coef.mode != MODE_RHS && !(o > Real(0))) bad |= ST_DENSITY;
         }

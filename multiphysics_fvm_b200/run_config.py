@@ -5,7 +5,8 @@
 
 Configurations: kh2d (2D sharp Kelvin-Helmholtz), kh3d (its 3D extrusion),
 rt3d (3D Rayleigh-Taylor), maxwell_sph (spherical pulse), heat_cyl
-(cylindrical hot spot).  Prints the device time per step.
+(cylindrical hot spot), batch_c3 (96 mixed grids in one batch).  Prints the
+device time per step; --autotune picks the z-march depth first.
 """
 from __future__ import annotations
 
@@ -42,6 +43,25 @@ def make(name: str, n: int, precision: str | None = None):
     return s, np.stack([U[k] for k in backend.VARIABLES[backend.physics_name(s["physics"])]])
 
 
+def run_batch(steps: int, warmup: int, autotune: bool, seed: int = 0):
+    """The batched configuration (setups/batch_mixed.py): 96 grids, per-grid dt."""
+    from .setups import batch_mixed
+    setups = batch_mixed.make_setups(seed=seed)
+    states = batch_mixed.initial_states(setups)
+    b = backend.Batch(setups)
+    for i, U in enumerate(states):
+        b[i].upload(U)
+        b[i].set_time(0.0, math.inf, float(setups[i]["time_config"]["CFL"]))
+    cells = sum(int(np.prod([s["grid_config"][k] for k in ("nx1", "nx2", "nx3")])) for s in setups)
+    tuned = b.autotune() if autotune else None
+    b.step(warmup)
+    ms = b.time_steps(steps)
+    st = max(b[i].status() for i in range(len(b)))
+    print(f"batch_c3 grids={len(b)} cells={cells} tiles={b.tiles()} autotune={tuned}: {ms / steps:.3f} ms/step, "
+          f"{cells * steps / (ms / 1e3):.4e} cell-updates/s, status={st}")
+    return cells * steps / (ms / 1e3)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("config")
@@ -49,13 +69,20 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--precision", default=None)
+    ap.add_argument("--autotune", action="store_true")
     a = ap.parse_args()
+    if a.config == "batch_c3":
+        run_batch(a.steps, a.warmup, a.autotune)
+        return
     s, U = make(a.config, a.n, a.precision)
     sim = backend.Simulation.from_setup(s)
     sim.upload(U)
     sim.set_time(0.0, math.inf, float(s["time_config"]["CFL"]))
+    tuned = sim.autotune() if a.autotune else None
     sim.step(a.warmup)
     ms = sim.time_steps(a.steps)
+    if tuned:
+        print(f"autotuned z-march depth {tuned[0]} ({tuned[1]:.3f} ms/step in the sweep)")
     print(f"{a.config} n={a.n} {s.get('precision')}: {ms / a.steps:.3f} ms/step, status={sim.status()}")
 
 
