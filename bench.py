@@ -222,10 +222,12 @@ def run_ours(args):
     if os.path.exists(pk_path):
         peaks = json.load(open(pk_path))
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "ns_stage_traffic.json")
+    traffic = None  # DRAM bytes per stage launch from the committed ncu capture (profiles/)
+    tp = os.path.join(ROOT, "profiles", "ns_stage_rt3d_256.md")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("bytes_per_launch_256")
+        for line in open(tp):
+            if "traffic_bytes_per_launch_256:" in line:
+                traffic = float(line.split("traffic_bytes_per_launch_256:")[1].split()[0])
 
     # end to end through the public API with host buffers: upload the float64
     # ghosted state from pinned memory, one step, download it again
