@@ -1,4 +1,5 @@
-"""ctypes binding of libfvm_b200.so (the C ABI declared in include/fvm.h).
+"""ctypes binding of libfvm_b200.so (the C ABI declared in include/fvm.h and
+include/fvm_closure.h).
 
 The library is built in-tree by ``python -m multiphysics_fvm_b200.build`` (or
 ``__graft_entry__.build()``).  There is no fallback: if the library or a CUDA
@@ -73,6 +74,27 @@ SIGNATURES = [
     ("fvm_batch_step", C.c_int, [_P, C.c_int, C.c_int]),
     ("fvm_batch_time_steps", C.c_int, [_P, C.c_int, C.c_int, _DP]),
     ("fvm_batch_autotune", C.c_int, [_P, C.POINTER(C.c_int), _DP]),
+    # learned closure (include/fvm_closure.h)
+    ("fvm_closure_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(_P)]),
+    ("fvm_closure_destroy", C.c_int, [_P]),
+    ("fvm_closure_set_norm", C.c_int, [_P, C.c_double, _DP, _DP, _DP, _DP]),
+    ("fvm_closure_set_weights", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p]),
+    ("fvm_closure_get_weights", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p]),
+    ("fvm_closure_get_grads", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p]),
+    ("fvm_closure_buffer", C.c_int, [_P, C.c_int, C.c_void_p, C.c_longlong, C.c_int]),
+    ("fvm_closure_features", C.c_int, [_P, C.c_void_p]),
+    ("fvm_closure_forward", C.c_int, [_P]),
+    ("fvm_closure_backward", C.c_int, [_P, C.c_void_p, C.c_double, _DP]),
+    ("fvm_closure_adam", C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_double]),
+    ("fvm_closure_train_step", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_double, _DP, C.c_double]),
+    ("fvm_closure_loss", C.c_int, [_P, _DP]),
+    ("fvm_closure_correct_dense", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, _DP,
+                                            C.POINTER(C.c_ulonglong)]),
+    ("fvm_closure_attach", C.c_int, [_P, _P, C.c_double]),
+    ("fvm_closure_switch_count", C.c_int, [_P, C.POINTER(C.c_ulonglong)]),
+    ("fvm_filter_state", C.c_int, [_P, C.c_int, C.c_void_p]),
+    ("fvm_upload_dense", C.c_int, [_P, C.c_void_p]),
+    ("fvm_download_dense", C.c_int, [_P, C.c_void_p]),
 ]
 
 _lib = None

@@ -1,0 +1,248 @@
+"""Training data, training and evaluation of the learned flux-correction
+closure on 3D Kelvin-Helmholtz (triply periodic [0,1]^3, the sharp profile
+extruded in x3 with seeded noise on all three velocity components, MUSCL
+minmod + HLL + SSPRK3, float32).
+
+Data: seeded fine runs at ``fine``^3 with a fixed step dt_c/f (f = the
+filter factor, dt_c the coarse step), box-filtered f^3 to the coarse grid.
+At every ``sample_every``-th coarse step the pair (U_bar(t), U_bar(t+dt_c))
+gives the defect D = U_bar(t+dt_c) - S_c(U_bar(t)) of one plain coarse step
+S_c; the network is trained so that dt_c * (-div dF) matches D (a-priori
+loss, per-variable weights 1/mean(D_q^2), so the loss of a zero correction is
+5).  Evaluation on held-out seeds: density L2 error at t_end against the
+filtered fine run for plain coarse, coarse + closure and plain 2x-coarse
+(filtered to the coarse grid), with the device time of each run.
+
+    python -m multiphysics_fvm_b200.closure_train --fine 256 --factor 4 \\
+        --train-seeds 32 --eval-seeds 8 --out closure.npz --report closure.json
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+from dataclasses import asdict, dataclass, field
+
+import numpy as np
+
+from . import backend
+from . import closure as CL
+from .grid.geometry import build_grid
+
+
+@dataclass
+class Config:
+    fine: int = 256
+    factor: int = 4
+    t_end: float = 1.0
+    dt_coarse: float = 2e-3
+    sample_every: int = 5
+    train_seeds: list = field(default_factory=lambda: list(range(32)))
+    eval_seeds: list = field(default_factory=lambda: list(range(1000, 1008)))
+    epochs: int = 3
+    lr: float = 1e-3
+    beta: float = 0.5
+    net_seed: int = 0
+
+    @property
+    def coarse(self) -> int:
+        return self.fine // self.factor
+
+    @property
+    def n_coarse_steps(self) -> int:
+        return int(round(self.t_end / self.dt_coarse))
+
+
+def kh_setup(n: int, seed: int):
+    from .setups import kelvin_helmholtz_sharp as kh
+    return kh.get_setup(n, n, n, seed=seed, precision="fp32", noise_all=True)
+
+
+def new_sim(n: int, seed: int, initial_state: bool = True):
+    s = kh_setup(n, seed)
+    sim = backend.Simulation.from_setup(s)
+    if initial_state:
+        g = build_grid(s["coordinate_system"], s["grid_config"])
+        U = s["physics"].allocate_u(s["grid_config"])
+        s["initial_conditions"]["initializer"](U, s["physical_parameters"], g, s["initial_conditions"]["parameters"])
+        sim.upload(U)
+    sim.set_time(0.0, math.inf, float(s["time_config"]["CFL"]))
+    return sim
+
+
+def generate(cfg: Config, seeds, log=print):
+    """Training pairs (U_bar, D) as CUDA tensors (N, 5, n, n, n)."""
+    import torch
+    f, nc = cfg.factor, cfg.coarse
+    coarse = new_sim(nc, 0, initial_state=False)
+    Us, Ds = [], []
+    for seed in seeds:
+        t0 = time.time()
+        fine = new_sim(cfg.fine, seed)
+        for m in range(cfg.n_coarse_steps):
+            take = m % cfg.sample_every == 0
+            if take:
+                ub0 = CL.filter_state(fine, f)
+            fine.step(f, dt=cfg.dt_coarse / f)
+            if take:
+                ub1 = CL.filter_state(fine, f)
+                CL.upload_dense(coarse, ub0)
+                coarse.step(1, dt=cfg.dt_coarse)
+                Ds.append(ub1 - CL.download_dense(coarse))
+                Us.append(ub0)
+        st = fine.status()
+        fine.close()
+        torch.cuda.synchronize()
+        log(f"seed {seed}: {len(Us)} pairs, status {st}, {time.time() - t0:.1f} s")
+        if st:
+            raise RuntimeError(f"fine run of seed {seed} reported status {st}")
+    coarse.close()
+    return torch.stack(Us), torch.stack(Ds)
+
+
+def normalisation(U, D, cfg: Config, gamma: float = 1.4):
+    """Feature mean/scale, output scales and loss weights from the data."""
+    import torch
+    rho = U[:, 0]
+    v = U[:, 1:4] / rho[:, None]
+    p = (gamma - 1.0) * (U[:, 4] - 0.5 * rho * (v * v).sum(1))
+    prim = torch.stack([rho, v[:, 0], v[:, 1], v[:, 2], p], 1)
+    mean = prim.mean(dim=(0, 2, 3, 4)).double().cpu().numpy()
+    scale = prim.std(dim=(0, 2, 3, 4)).double().cpu().numpy()
+    rms = D.double().pow(2).mean(dim=(0, 2, 3, 4)).sqrt().cpu().numpy()
+    h = 1.0 / cfg.coarse
+    out_scale = rms * h / cfg.dt_coarse
+    weight = 1.0 / (rms * rms)
+    return dict(gamma=gamma, in_mean=mean, in_scale=np.maximum(scale, 1e-6), out_scale=out_scale,
+                loss_weight=weight)
+
+
+def apriori_loss(net: CL.Closure, U, D, cfg: Config) -> float:
+    """Mean a-priori loss over samples (5 = no improvement over the plain step)."""
+    h = (1.0 / cfg.coarse,) * 3
+    tot = 0.0
+    for i in range(U.shape[0]):
+        net.features(U[i])
+        net.forward()
+        net.backward(D[i], cfg.dt_coarse, h)
+        tot += net.loss()
+    return tot / U.shape[0]
+
+
+def train(cfg: Config, U, D, log=print, net: CL.Closure | None = None):
+    import torch
+    nc = cfg.coarse
+    if net is None:
+        net = CL.Closure((nc, nc, nc), seed=cfg.net_seed)
+    nrm = normalisation(U, D, cfg)
+    net.set_norm(**nrm)
+    h = (1.0 / nc,) * 3
+    g = torch.Generator().manual_seed(cfg.net_seed)
+    curve = []
+    t0 = time.time()
+    it = 0
+    for ep in range(cfg.epochs):
+        order = torch.randperm(U.shape[0], generator=g).tolist()
+        run = 0.0
+        for k, i in enumerate(order):
+            net.train_step(U[i], D[i], cfg.dt_coarse, h, cfg.lr)
+            run += net.loss()
+            it += 1
+            if (k + 1) % 200 == 0 or k + 1 == len(order):
+                curve.append((it, run / ((k % 200) + 1)))
+                run = 0.0
+        log(f"epoch {ep}: loss {curve[-1][1]:.4f} ({time.time() - t0:.1f} s)")
+    return net, curve, time.time() - t0
+
+
+def _rho_err(a, b) -> float:
+    return float((a[0] - b[0]).double().pow(2).mean().sqrt().item())
+
+
+def evaluate(cfg: Config, net: CL.Closure, seeds, log=print):
+    """Per-seed density L2 errors at t_end and device times (ms) per run."""
+    f, nc, n = cfg.factor, cfg.coarse, cfg.n_coarse_steps
+    nm = cfg.fine // 2
+    rows = []
+    plain = new_sim(nc, 0, initial_state=False)
+    closed = new_sim(nc, 0, initial_state=False)
+    net.attach(closed, beta=cfg.beta)
+    mid = new_sim(nm, 0, initial_state=False)
+    for seed in seeds:
+        fine = new_sim(cfg.fine, seed)
+        ic_c = CL.filter_state(fine, f)
+        ic_m = CL.filter_state(fine, 2)
+        ms_fine = _timed(fine, n * f, cfg.dt_coarse / f)
+        ref = CL.filter_state(fine, f)
+        fine.close()
+        out = {"seed": seed, "ms_fine": ms_fine}
+        sw0 = CL.Closure.switch_count(closed)
+        for name, sim, ic, steps, dt, back in (("plain", plain, ic_c, n, cfg.dt_coarse, 1),
+                                               ("closure", closed, ic_c, n, cfg.dt_coarse, 1),
+                                               ("plain_2x", mid, ic_m, 2 * n, cfg.dt_coarse / 2, 2)):
+            CL.upload_dense(sim, ic)
+            sim.set_time(0.0, math.inf, 0.4)
+            out[f"ms_{name}"] = _timed(sim, steps, dt)
+            res = CL.filter_state(sim, back) if back > 1 else CL.download_dense(sim)
+            out[f"err_{name}"] = _rho_err(res, ref)
+            out[f"status_{name}"] = sim.status()
+        out["switched"] = CL.Closure.switch_count(closed) - sw0
+        rows.append(out)
+        log(json.dumps(out))
+    for s in (plain, closed, mid):
+        s.close()
+    return rows
+
+
+def _timed(sim, steps: int, dt: float) -> float:
+    """Advance `steps` fixed steps of size dt; device time in ms."""
+    from . import _lib as L
+    L.check(sim._lib.fvm_set_dt(sim._h, float(dt)), "fvm_set_dt")
+    return sim.time_steps(steps, fixed_dt=True)
+
+
+def summarise(rows):
+    keys = ("err_plain", "err_closure", "err_plain_2x", "ms_plain", "ms_closure", "ms_plain_2x", "ms_fine")
+    return {k: float(np.mean([r[k] for r in rows])) for k in keys}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--fine", type=int, default=256)
+    ap.add_argument("--factor", type=int, default=4)
+    ap.add_argument("--t-end", type=float, default=1.0)
+    ap.add_argument("--dt-coarse", type=float, default=2e-3)
+    ap.add_argument("--sample-every", type=int, default=5)
+    ap.add_argument("--train-seeds", type=int, default=32)
+    ap.add_argument("--eval-seeds", type=int, default=8)
+    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--beta", type=float, default=0.5)
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--report", required=True)
+    a = ap.parse_args(argv)
+    cfg = Config(fine=a.fine, factor=a.factor, t_end=a.t_end, dt_coarse=a.dt_coarse, sample_every=a.sample_every,
+                 train_seeds=list(range(a.train_seeds)), eval_seeds=list(range(1000, 1000 + a.eval_seeds)),
+                 epochs=a.epochs, lr=a.lr, beta=a.beta)
+    t0 = time.time()
+    U, D = generate(cfg, cfg.train_seeds)
+    t_gen = time.time() - t0
+    nh = max(1, U.shape[0] // 10)
+    net, curve, t_train = train(cfg, U, D)
+    # held-out a-priori check on the eval seeds' first pairs
+    Uv, Dv = generate(Config(**{**asdict(cfg), "t_end": cfg.t_end / 2}), cfg.eval_seeds[:2])
+    apri = apriori_loss(net, Uv, Dv, cfg)
+    apri_train = apriori_loss(net, U[:nh], D[:nh], cfg)
+    rows = evaluate(cfg, net, cfg.eval_seeds)
+    rep = {"config": asdict(cfg), "pairs": int(U.shape[0]), "seconds_generate": t_gen, "seconds_train": t_train,
+           "loss_curve": curve, "apriori_loss_heldout": apri, "apriori_loss_train_subset": apri_train,
+           "apriori_loss_plain": 5.0, "eval": rows, "summary": summarise(rows)}
+    net.save(a.out, meta={"config": asdict(cfg), "summary": rep["summary"]})
+    with open(a.report, "w") as fh:
+        json.dump(rep, fh, indent=1)
+    print(json.dumps(rep["summary"]))
+
+
+if __name__ == "__main__":
+    main()

@@ -12,6 +12,8 @@
 #include <vector>
 
 #include "../../include/fvm.h"
+#include "../../include/fvm_closure.h"
+#include "closure_host.h"
 #include "fvm_aux.cuh"
 #include "launch.cuh"
 
@@ -31,6 +33,12 @@ int fail(int code, const std::string& msg) {
     cudaError_t e_ = (x);                                                                        \
     if (e_ != cudaSuccess) return fail(FVM_E_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+}  // namespace
+
+int fvm::set_error(int code, const std::string& msg) { return fail(code, msg); }
+
+namespace {
 
 // Host copy of the per-axis metric tables (float64), built with the
 // reference's expressions (src/grid/geometry.py:37-171).
@@ -108,6 +116,9 @@ struct fvm_handle {
   double max_inv_l2 = 0.0, const_rate = 0.0;
   int zchunk = 64;
   long long device_bytes = 0;
+  fvm_closure* closure = nullptr;  // learned flux correction run inside every step
+  double closure_beta = 0.5;
+  unsigned long long* closure_nswitch = nullptr;
 };
 
 namespace {
@@ -368,6 +379,12 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
   const int cmode = dt_mode == 1 ? 1 : (state_dt ? 0 : 2);
   clock_kernel<<<1, 1, 0, h->stream>>>(h->clk, cmode, h->max_inv_l2, h->const_rate, h->status);
   FVM_CK(cudaGetLastError());
+  if (h->closure) {
+    // face corrections from the step's base state (periodic: no ghosts read)
+    cudaError_t e = closure::enqueue_infer(h->closure, static_cast<const float*>(h->U[0]), h->lay,
+                                           (float)h->d.params[0], h->stream);
+    if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("closure: ") + cudaGetErrorString(e));
+  }
   for (const StageDef& sd : stage_table(h->d.integrator)) {
     cudaError_t e = launch_bc(h, sd.in, true);
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
@@ -375,6 +392,16 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
     if ((rc = mark(pf ? pf->a : nullptr))) return rc;
     e = h->f64 ? launch_stage<double>(h, sd, false) : launch_stage<float>(h, sd, false);
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("stage kernel: ") + cudaGetErrorString(e));
+    if (h->closure) {
+      // d(out)/d(dt k) of the stage combination
+      const double coef = sd.mode == MODE_EULER ? 1.0 : (sd.mode == MODE_AXPY ? sd.ca : sd.cb);
+      const double hh[3] = {(h->d.x1_max - h->d.x1_min) / h->d.nx1, (h->d.x2_max - h->d.x2_min) / h->d.nx2,
+                            (h->d.x3_max - h->d.x3_min) / h->d.nx3};
+      e = closure::enqueue_fix(h->closure, static_cast<const float*>(h->U[sd.in]), static_cast<float*>(h->U[sd.out]),
+                               h->lay, (float)h->d.params[0], (float)coef, (float)h->closure_beta, hh, h->clk,
+                               h->closure_nswitch, h->stream);
+      if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("closure correction: ") + cudaGetErrorString(e));
+    }
     if ((rc = close(true))) return rc;
     if ((rc = mark(pf ? pf->a : nullptr))) return rc;
   }
@@ -543,6 +570,7 @@ int fvm_destroy(fvm_handle* h) {
   if (h->totals_dev) cudaFree(h->totals_dev);
   if (h->stage_dev) cudaFree(h->stage_dev);
   if (h->stage_host) cudaFreeHost(h->stage_host);
+  if (h->closure_nswitch) cudaFree(h->closure_nswitch);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return FVM_OK;
@@ -1308,5 +1336,69 @@ int fvm_batch_autotune(fvm_batch* b, int* best_zchunk, double* best_ms) {
   if (best_ms) *best_ms = bt / 3.0;
   return FVM_OK;
 }
+
+}  // extern "C"
+
+// ------------------------------------------------------------ closure hook ----
+extern "C" {
+
+int fvm_closure_attach(fvm_handle* h, fvm_closure* c, double beta) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  if (c) {
+    const fvm_desc& d = h->d;
+    if (d.physics != FVM_NAVIER_STOKES || h->f64 || d.coords != FVM_CARTESIAN)
+      return fail(FVM_E_INVALID, "closure: needs a float32 cartesian navier_stokes handle");
+    if (d.integrator != FVM_RK3_SSP && d.integrator != FVM_EULER_EXPLICIT)
+      return fail(FVM_E_INVALID, "closure: integrator must be rk3_ssp or euler_explicit");
+    for (int q = 0; q < h->nv; ++q)
+      for (int s = 0; s < 6; ++s)
+        if (d.bc_kind[q][s] != FVM_BC_PERIODIC) return fail(FVM_E_INVALID, "closure: every face must be periodic");
+    if (!closure::grid_matches(c, d.nx1, d.nx2, d.nx3)) return fail(FVM_E_INVALID, "closure: grid size differs");
+    if (!(beta >= 0.0)) return fail(FVM_E_INVALID, "closure: beta must be >= 0");
+    if (!h->closure_nswitch) {
+      FVM_CK(cudaMalloc(&h->closure_nswitch, sizeof(unsigned long long)));
+    }
+    FVM_CK(cudaMemset(h->closure_nswitch, 0, sizeof(unsigned long long)));
+  }
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  for (auto& g : h->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  h->closure = c;
+  h->closure_beta = beta;
+  return FVM_OK;
+}
+
+int fvm_closure_switch_count(fvm_handle* h, unsigned long long* out) {
+  if (!h || !out) return fail(FVM_E_INVALID, "null argument");
+  *out = 0;
+  if (!h->closure_nswitch) return FVM_OK;
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  FVM_CK(cudaMemcpy(out, h->closure_nswitch, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  return FVM_OK;
+}
+
+int fvm_filter_state(fvm_handle* h, int factor, float* coarse_dense_dev) {
+  if (!h || !coarse_dense_dev) return fail(FVM_E_INVALID, "null argument");
+  if (h->f64) return fail(FVM_E_INVALID, "filter: float32 handles only");
+  const Layout& L = h->lay;
+  if (factor < 1 || L.nx % factor || L.ny % factor || L.nz % factor)
+    return fail(FVM_E_INVALID, "filter: factor must divide every grid dimension");
+  FVM_CK(closure::launch_box_filter(static_cast<const float*>(h->U[0]), L, h->nv, factor, coarse_dense_dev, h->nsm,
+                                    h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+static int dense_copy(fvm_handle* h, float* dense, int to_state) {
+  if (!h || !dense) return fail(FVM_E_INVALID, "null argument");
+  if (h->f64) return fail(FVM_E_INVALID, "dense copy: float32 handles only");
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  FVM_CK(closure::launch_dense_copy(static_cast<float*>(h->U[0]), h->lay, h->nv, dense, to_state, h->nsm, h->stream));
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+int fvm_upload_dense(fvm_handle* h, const float* dense_dev) { return dense_copy(h, const_cast<float*>(dense_dev), 1); }
+int fvm_download_dense(fvm_handle* h, float* dense_dev) { return dense_copy(h, dense_dev, 0); }
 
 }  // extern "C"

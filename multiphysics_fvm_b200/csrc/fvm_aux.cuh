@@ -90,13 +90,6 @@ __global__ void transpose_kernel(const double* __restrict__ hsrc, double* __rest
   }
 }
 
-// Device-resident time-loop scalars.
-struct Clock {
-  double t, t_end, dt, cfl, dt_fixed;
-  long long steps;
-  int active;
-  unsigned long long red[2];  // running maxima (bit patterns of non-negative doubles)
-};
 
 // ------------------------------------------------------------- batches ----
 // Per-instance data of the batched auxiliary kernels.

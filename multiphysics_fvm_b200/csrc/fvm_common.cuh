@@ -233,6 +233,14 @@ __device__ __forceinline__ R muscl_slope(R fm, R f0, R fp, R L) {
   }
 }
 
+// Device-resident time-loop scalars.
+struct Clock {
+  double t, t_end, dt, cfl, dt_fixed;
+  long long steps;
+  int active;
+  unsigned long long red[2];  // running maxima (bit patterns of non-negative doubles)
+};
+
 // --------------------------------------------------------- PTX helpers ----
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));

@@ -12,11 +12,15 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "fvm.h")
+HEADERS = sorted(os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))
+                 if f.endswith(".h"))
 
 
 def declared_functions():
-    src = open(HEADER).read()
-    return sorted(set(re.findall(r"^int\s+(fvm_\w+)\s*\(", src, flags=re.M)))
+    names = set()
+    for h in HEADERS:
+        names |= set(re.findall(r"^int\s+(fvm_\w+)\s*\(", open(h).read(), flags=re.M))
+    return sorted(names)
 
 
 def test_library_exports_every_declared_symbol():
