@@ -49,6 +49,20 @@ def apply_ics(U: dict, params: dict, grid: dict, ics: dict) -> None:
     ics["initializer"](U, params, grid, ics["parameters"])
 
 
+def _attach_closure(sim, spec):
+    """Optional learned flux correction: ``setup["closure"] = {"weights": path
+    or closure.Closure, "beta": 0.5}`` (navier_stokes, fp32, cartesian,
+    periodic, rk3_ssp or euler_explicit)."""
+    if not spec:
+        return
+    from . import closure
+    net = spec["weights"]
+    if not isinstance(net, closure.Closure):
+        net = closure.Closure(sim.n)
+        net.load(spec["weights"])
+    net.attach(sim, beta=float(spec.get("beta", 0.5)))
+
+
 def run(setup: dict, verbose: bool = True):
     """Run a setup (src/solver.py:88-151) with the state resident on the device.
     Returns the Simulation (its final state via ``download()``)."""
@@ -67,6 +81,7 @@ def run(setup: dict, verbose: bool = True):
     sim = backend.Simulation.from_setup(setup)
     sim.upload(U)
     sim.set_time(t_start, t_end, cfl)
+    _attach_closure(sim, setup.get("closure"))
     limit = n_steps if n_steps is not None else None
     n = 0
     while True:
