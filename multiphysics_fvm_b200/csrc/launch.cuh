@@ -14,11 +14,15 @@ namespace fvm {
 template <typename Real, bool VISC>
 constexpr int ns_tile_ty() { return std::is_same<Real, double>::value ? (VISC ? 4 : 8) : (VISC ? 6 : 8); }
 template <typename Real, bool VISC>
-constexpr int ns_min_blocks() { return std::is_same<Real, double>::value ? 1 : 2; }
+constexpr int ns_min_blocks() { return std::is_same<Real, double>::value ? 1 : (VISC ? 2 : 3); }
 
 template <typename K>
 static cudaError_t prepare_kernel(K kern, int threads, int bytes, int* blocks_per_sm) {
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  // all of the unified L1/shared array as shared memory: the ring planes are
+  // the blocks' working set, so more resident blocks beat a larger L1
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, threads, bytes);
   if (e != cudaSuccess) return e;
