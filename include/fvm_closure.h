@@ -53,6 +53,14 @@ int fvm_closure_destroy(fvm_closure* c);
 int fvm_closure_set_norm(fvm_closure* c, double gamma, const double in_mean[5], const double in_scale[5],
                          const double out_scale[5], const double loss_weight[5]);
 
+/* Bound on the per-stage corrections: 0 = each face correction clipped to
+ * +-beta*max(|v_a|+c)*|dU| only; 1 = that clip, then the flux-corrected
+ * transport limiter (Zalesak): every face transfer is scaled so that the
+ * corrected stage result stays inside the min/max of the plain stage result
+ * over the cell and its six neighbours (no new extrema).  Set before
+ * fvm_closure_attach (an attached step graph keeps the mode it was built with). */
+int fvm_closure_set_limiter(fvm_closure* c, int fct);
+
 /* layer in 1..3.  set_* resets that layer's Adam moments. */
 int fvm_closure_set_weights(fvm_closure* c, int layer, const float* w_host, const float* b_host);
 int fvm_closure_get_weights(fvm_closure* c, int layer, float* w_host, float* b_host);

@@ -78,6 +78,7 @@ SIGNATURES = [
     ("fvm_closure_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(_P)]),
     ("fvm_closure_destroy", C.c_int, [_P]),
     ("fvm_closure_set_norm", C.c_int, [_P, C.c_double, _DP, _DP, _DP, _DP]),
+    ("fvm_closure_set_limiter", C.c_int, [_P, C.c_int]),
     ("fvm_closure_set_weights", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p]),
     ("fvm_closure_get_weights", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p]),
     ("fvm_closure_get_grads", C.c_int, [_P, C.c_int, C.c_void_p, C.c_void_p]),

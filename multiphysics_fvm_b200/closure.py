@@ -66,6 +66,7 @@ class Closure:
         self._h = h
         self.npos = self.n[0] * self.n[1] * self.n[2]
         self.norm = None
+        self.fct = False
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -89,6 +90,12 @@ class Closure:
                 "fvm_closure_set_norm")
         self.norm = {"gamma": float(gamma), "in_mean": arrs[0].tolist(), "in_scale": arrs[1].tolist(),
                      "out_scale": arrs[2].tolist(), "loss_weight": arrs[3].tolist()}
+
+    def set_limiter(self, fct: bool):
+        """True: flux-corrected transport bound on top of the face clip (no
+        new extrema); set before ``attach``."""
+        L.check(self._lib.fvm_closure_set_limiter(self._h, 1 if fct else 0), "fvm_closure_set_limiter")
+        self.fct = bool(fct)
 
     def get_weights(self):
         out = []

@@ -42,6 +42,7 @@ class Config:
     eval_seeds: list = field(default_factory=lambda: list(range(1000, 1008)))
     epochs: int = 3
     lr: float = 1e-3
+    defect_steps: int = 1   # k: target = (U_bar(t + k dt_c) - S_c^k(U_bar(t))) / k
     beta: float = 0.5
     net_seed: int = 0
 
@@ -72,25 +73,33 @@ def new_sim(n: int, seed: int, initial_state: bool = True):
 
 
 def generate(cfg: Config, seeds, log=print):
-    """Training pairs (U_bar, D) as CUDA tensors (N, 5, n, n, n)."""
+    """Training pairs (U_bar, D) as CUDA tensors (N, 5, n, n, n).  With k =
+    defect_steps > 1 the defect is averaged over k coarse steps, which spreads
+    the coarse scheme's own relaxation of a freshly filtered state over the
+    window and keeps the persistent part that a correction can carry."""
     import torch
-    f, nc = cfg.factor, cfg.coarse
+    f, nc, k = cfg.factor, cfg.coarse, cfg.defect_steps
+    if k > cfg.sample_every:
+        raise ValueError("defect_steps must not exceed sample_every")
     coarse = new_sim(nc, 0, initial_state=False)
     Us, Ds = [], []
     for seed in seeds:
         t0 = time.time()
         fine = new_sim(cfg.fine, seed)
-        for m in range(cfg.n_coarse_steps):
-            take = m % cfg.sample_every == 0
-            if take:
-                ub0 = CL.filter_state(fine, f)
+        pending = None
+        for m in range(cfg.n_coarse_steps + 1):
+            if pending is not None and m == pending[0]:
+                ubk = CL.filter_state(fine, f)
+                CL.upload_dense(coarse, pending[1])
+                coarse.step(k, dt=cfg.dt_coarse)
+                Ds.append((ubk - CL.download_dense(coarse)) / k)
+                Us.append(pending[1])
+                pending = None
+            if m == cfg.n_coarse_steps:
+                break
+            if m % cfg.sample_every == 0 and m + k <= cfg.n_coarse_steps:
+                pending = (m + k, CL.filter_state(fine, f))
             fine.step(f, dt=cfg.dt_coarse / f)
-            if take:
-                ub1 = CL.filter_state(fine, f)
-                CL.upload_dense(coarse, ub0)
-                coarse.step(1, dt=cfg.dt_coarse)
-                Ds.append(ub1 - CL.download_dense(coarse))
-                Us.append(ub0)
         st = fine.status()
         fine.close()
         torch.cuda.synchronize()
@@ -160,36 +169,53 @@ def _rho_err(a, b) -> float:
     return float((a[0] - b[0]).double().pow(2).mean().sqrt().item())
 
 
-def evaluate(cfg: Config, net: CL.Closure, seeds, log=print):
-    """Per-seed density L2 errors at t_end and device times (ms) per run."""
+def evaluate(cfg: Config, net: CL.Closure, seeds, betas=None, checkpoints: int = 4, log=print):
+    """Per seed: density L2 error against the filtered fine run at
+    ``checkpoints`` equally spaced times up to t_end, and the device time (ms)
+    of each run, for plain coarse, coarse + closure at each clip factor in
+    ``betas`` and plain 2x-coarse (filtered to the coarse grid)."""
+    import torch
+    betas = [cfg.beta] if betas is None else list(betas)
     f, nc, n = cfg.factor, cfg.coarse, cfg.n_coarse_steps
+    seg = n // checkpoints
     nm = cfg.fine // 2
     rows = []
     plain = new_sim(nc, 0, initial_state=False)
     closed = new_sim(nc, 0, initial_state=False)
-    net.attach(closed, beta=cfg.beta)
     mid = new_sim(nm, 0, initial_state=False)
     for seed in seeds:
         fine = new_sim(cfg.fine, seed)
         ic_c = CL.filter_state(fine, f)
         ic_m = CL.filter_state(fine, 2)
-        ms_fine = _timed(fine, n * f, cfg.dt_coarse / f)
-        ref = CL.filter_state(fine, f)
+        refs, ms_fine = [], 0.0
+        for _ in range(checkpoints):
+            ms_fine += _timed(fine, seg * f, cfg.dt_coarse / f)
+            refs.append(CL.filter_state(fine, f))
         fine.close()
-        out = {"seed": seed, "ms_fine": ms_fine}
-        sw0 = CL.Closure.switch_count(closed)
-        for name, sim, ic, steps, dt, back in (("plain", plain, ic_c, n, cfg.dt_coarse, 1),
-                                               ("closure", closed, ic_c, n, cfg.dt_coarse, 1),
-                                               ("plain_2x", mid, ic_m, 2 * n, cfg.dt_coarse / 2, 2)):
+        out = {"seed": seed, "t": [cfg.dt_coarse * seg * (c + 1) for c in range(checkpoints)], "ms_fine": ms_fine}
+        runs = [("plain", plain, None, ic_c, 1, cfg.dt_coarse, 1)]
+        runs += [(f"closure_b{b:g}", closed, b, ic_c, 1, cfg.dt_coarse, 1) for b in betas]
+        runs += [("plain_2x", mid, None, ic_m, 2, cfg.dt_coarse / 2, 2)]
+        for name, sim, beta, ic, mult, dt, back in runs:
+            if beta is not None:
+                net.attach(sim, beta=beta)  # resets the switch counter
             CL.upload_dense(sim, ic)
+            sim.clear_status()
             sim.set_time(0.0, math.inf, 0.4)
-            out[f"ms_{name}"] = _timed(sim, steps, dt)
-            res = CL.filter_state(sim, back) if back > 1 else CL.download_dense(sim)
-            out[f"err_{name}"] = _rho_err(res, ref)
-            out[f"status_{name}"] = sim.status()
-        out["switched"] = CL.Closure.switch_count(closed) - sw0
+            errs, ms = [], 0.0
+            for c in range(checkpoints):
+                ms += _timed(sim, seg * mult, dt)
+                res = CL.filter_state(sim, back) if back > 1 else CL.download_dense(sim)
+                errs.append(_rho_err(res, refs[c]))
+            rec = {"err": errs, "ms": ms, "status": sim.status()}
+            if beta is not None:
+                rec["switched"] = CL.Closure.switch_count(sim)
+                rec["beta"] = beta
+            out[name] = rec
         rows.append(out)
         log(json.dumps(out))
+        del refs
+        torch.cuda.empty_cache()
     for s in (plain, closed, mid):
         s.close()
     return rows
@@ -203,8 +229,13 @@ def _timed(sim, steps: int, dt: float) -> float:
 
 
 def summarise(rows):
-    keys = ("err_plain", "err_closure", "err_plain_2x", "ms_plain", "ms_closure", "ms_plain_2x", "ms_fine")
-    return {k: float(np.mean([r[k] for r in rows])) for k in keys}
+    """Mean over seeds of the final-time error and the device time of each run."""
+    names = [k for k in rows[0] if isinstance(rows[0][k], dict)]
+    out = {"ms_fine": float(np.mean([r["ms_fine"] for r in rows]))}
+    for k in names:
+        out[f"err_{k}"] = float(np.mean([r[k]["err"][-1] for r in rows]))
+        out[f"ms_{k}"] = float(np.mean([r[k]["ms"] for r in rows]))
+    return out
 
 
 def main(argv=None):
@@ -219,23 +250,43 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=3)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--beta", type=float, default=0.5)
-    ap.add_argument("--out", required=True)
+    ap.add_argument("--defect-steps", type=int, default=1)
+    ap.add_argument("--betas", default="", help="comma-separated clip factors to evaluate (default: --beta)")
+    ap.add_argument("--checkpoints", type=int, default=4)
+    ap.add_argument("--weights", default="", help="evaluate these weights instead of training")
+    ap.add_argument("--fct", action="store_true", help="flux-corrected transport bound on the corrections")
+    ap.add_argument("--out", default="")
     ap.add_argument("--report", required=True)
     a = ap.parse_args(argv)
     cfg = Config(fine=a.fine, factor=a.factor, t_end=a.t_end, dt_coarse=a.dt_coarse, sample_every=a.sample_every,
                  train_seeds=list(range(a.train_seeds)), eval_seeds=list(range(1000, 1000 + a.eval_seeds)),
-                 epochs=a.epochs, lr=a.lr, beta=a.beta)
+                 epochs=a.epochs, lr=a.lr, beta=a.beta, defect_steps=a.defect_steps)
+    betas = [float(b) for b in a.betas.split(",") if b] or [cfg.beta]
+    if a.weights:
+        net = CL.Closure((cfg.coarse,) * 3)
+        meta = net.load(a.weights)
+        net.set_limiter(a.fct)
+        rows = evaluate(cfg, net, cfg.eval_seeds, betas, a.checkpoints)
+        rep = {"config": asdict(cfg), "fct": a.fct, "weights": a.weights, "weights_meta": meta, "eval": rows,
+               "summary": summarise(rows)}
+        with open(a.report, "w") as fh:
+            json.dump(rep, fh, indent=1)
+        print(json.dumps(rep["summary"]))
+        return
+    if not a.out:
+        ap.error("--out is required when training")
     t0 = time.time()
     U, D = generate(cfg, cfg.train_seeds)
     t_gen = time.time() - t0
     nh = max(1, U.shape[0] // 10)
     net, curve, t_train = train(cfg, U, D)
+    net.set_limiter(a.fct)
     # held-out a-priori check on the eval seeds' first pairs
     Uv, Dv = generate(Config(**{**asdict(cfg), "t_end": cfg.t_end / 2}), cfg.eval_seeds[:2])
     apri = apriori_loss(net, Uv, Dv, cfg)
     apri_train = apriori_loss(net, U[:nh], D[:nh], cfg)
-    rows = evaluate(cfg, net, cfg.eval_seeds)
-    rep = {"config": asdict(cfg), "pairs": int(U.shape[0]), "seconds_generate": t_gen, "seconds_train": t_train,
+    rows = evaluate(cfg, net, cfg.eval_seeds, betas, a.checkpoints)
+    rep = {"config": asdict(cfg), "fct": a.fct, "pairs": int(U.shape[0]), "seconds_generate": t_gen, "seconds_train": t_train,
            "loss_curve": curve, "apriori_loss_heldout": apri, "apriori_loss_train_subset": apri_train,
            "apriori_loss_plain": 5.0, "eval": rows, "summary": summarise(rows)}
     net.save(a.out, meta={"config": asdict(cfg), "summary": rep["summary"]})

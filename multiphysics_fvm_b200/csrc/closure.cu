@@ -63,6 +63,8 @@ struct fvm_closure {
   float out_scale[5] = {1, 1, 1, 1, 1}, loss_w[5] = {1, 1, 1, 1, 1};
   int zc_conv = 1, zc_wg = 1;
   unsigned* status = nullptr;  // ST_TMA_TIMEOUT when a tensor-core wait gave up
+  int fct = 0;                 // 1: flux-corrected transport bound on the corrections
+  float* ratio = nullptr;      // FCT fractions [10][cells]
 };
 
 namespace {
@@ -227,7 +229,20 @@ FixArgs fix_args(fvm_closure* c, const float* uin, float* uout, const Layout& la
   a.clk = clk;
   a.dt_host = dt;
   a.nswitch = nswitch;
+  a.ratio = c->ratio;
   return a;
+}
+
+// The correction of one stage: clip-only, or the two FCT passes.
+cudaError_t launch_fix(fvm_closure* c, const FixArgs& a, cudaStream_t s) {
+  if (c->fct) {
+    fct_ratio_kernel<<<4 * c->nsm, 256, 0, s>>>(a);
+    CL_RET(cudaGetLastError());
+    fct_apply_kernel<<<4 * c->nsm, 256, 0, s>>>(a);
+  } else {
+    closure_fix_kernel<<<4 * c->nsm, 256, 0, s>>>(a);
+  }
+  return cudaGetLastError();
 }
 
 template <typename T>
@@ -292,8 +307,7 @@ cudaError_t enqueue_fix(fvm_closure* c, const float* uin, float* uout, const Lay
                         float beta, const double h[3], const Clock* clk, unsigned long long* nswitch,
                         cudaStream_t s) {
   const FixArgs a = fix_args(c, uin, uout, lay, gamma, coef, beta, h, clk, 0.f, nswitch);
-  closure_fix_kernel<<<4 * c->nsm, 256, 0, s>>>(a);
-  return cudaGetLastError();
+  return launch_fix(c, a, s);
 }
 }  // namespace closure
 }  // namespace fvm
@@ -330,6 +344,7 @@ int fvm_closure_create(int n1, int n2, int n3, unsigned long long seed, fvm_clos
   if (!rc) rc = dalloc(&c->g2, np * C_HID);
   if (!rc) rc = dalloc(&c->g1, np * C_HID);
   if (!rc) rc = dalloc(&c->e, np * 5);
+  if (!rc) rc = dalloc(&c->ratio, np * 10);
   if (!rc) rc = dalloc(&c->partial, c->partial_elems);
   if (!rc) rc = dalloc(&c->loss_part, (size_t)c->loss_blocks);
   if (!rc) rc = dalloc(&c->loss_dev, 1);
@@ -377,7 +392,7 @@ int fvm_closure_destroy(fvm_closure* c) {
   if (!c) return FVM_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   void* ptrs[] = {c->x0,      c->a1,        c->a2,       c->z3,      c->g3,    c->g2,
-                  c->g1,      c->e,         c->partial,  c->loss_part, c->loss_dev, c->status};
+                  c->g1,      c->e,         c->partial,  c->loss_part, c->loss_dev, c->status, c->ratio};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int l = 0; l < NLAYER; ++l) {
@@ -405,6 +420,14 @@ int fvm_closure_set_norm(fvm_closure* c, double gamma, const double in_mean[5], 
     c->out_scale[q] = (float)out_scale[q];
     c->loss_w[q] = (float)loss_weight[q];
   }
+  return FVM_OK;
+}
+
+int fvm_closure_set_limiter(fvm_closure* c, int fct) {
+  if (int rc = check(c)) return rc;
+  if (fct != 0 && fct != 1) return set_error(FVM_E_INVALID, "closure limiter: 0 (face clip) or 1 (face clip + FCT)");
+  CL_CK(cudaStreamSynchronize(c->stream));
+  c->fct = fct;
   return FVM_OK;
 }
 
@@ -529,8 +552,7 @@ int fvm_closure_correct_dense(fvm_closure* c, const float* uin_dense_dev, float*
   cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), c->stream);
   const FixArgs a = fix_args(c, uin_dense_dev, uout_dense_dev, dense_layout(c->n1, c->n2, c->n3), c->gamma,
                              (float)coef, (float)beta, h, nullptr, (float)dt, cnt);
-  closure_fix_kernel<<<4 * c->nsm, 256, 0, c->stream>>>(a);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_fix(c, a, c->stream);
   unsigned long long v = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&v, cnt, sizeof(v), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

@@ -774,6 +774,7 @@ struct FixArgs {
   const Clock* clk;   // dt and the active flag of the solver clock, or null
   float dt_host;      // dt when clk is null
   unsigned long long* nswitch;
+  float* ratio;       // flux-corrected transport fractions [10][cells] (fct mode)
 };
 __device__ __forceinline__ void load_cell(const FixArgs& a, int i, int j, int k, float* u) {
 #pragma unroll
@@ -787,50 +788,148 @@ __device__ __forceinline__ float wave_speed(const float* u, int ax, float gamma)
   const float va = ax == 0 ? v1 : (ax == 1 ? v2 : v3);
   return fabsf(va) + c;
 }
+// Clipped face corrections of cell c: Fp[ax][q] on its +x_ax face, Fm[ax][q]
+// on its -x_ax face (the +face of the neighbour below), and the dense
+// indices of the six neighbours (nb[ax][0] = -e_ax, nb[ax][1] = +e_ax).
+__device__ __forceinline__ void face_corrections(const FixArgs& a, const int c[3], long long p, float Fp[3][5],
+                                                 float Fm[3][5], long long nb[3][2]) {
+  const Layout& L = a.lay;
+  const int dims[3] = {L.nx, L.ny, L.nz};
+  float u0[5];
+  load_cell(a, c[0], c[1], c[2], u0);
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    int cp[3] = {c[0], c[1], c[2]}, cm[3] = {c[0], c[1], c[2]};
+    cp[ax] = (c[ax] + 1) % dims[ax];
+    cm[ax] = (c[ax] + dims[ax] - 1) % dims[ax];
+    float up[5], um[5];
+    load_cell(a, cp[0], cp[1], cp[2], up);
+    load_cell(a, cm[0], cm[1], cm[2], um);
+    const float s0 = wave_speed(u0, ax, a.gamma);
+    const float sp = fmaxf(s0, wave_speed(up, ax, a.gamma));
+    const float sm = fmaxf(s0, wave_speed(um, ax, a.gamma));
+    nb[ax][0] = ((long long)cm[2] * L.ny + cm[1]) * L.nx + cm[0];
+    nb[ax][1] = ((long long)cp[2] * L.ny + cp[1]) * L.nx + cp[0];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const float bp = a.beta * sp * fabsf(up[q] - u0[q]);
+      const float bm = a.beta * sm * fabsf(u0[q] - um[q]);
+      Fp[ax][q] = fminf(fmaxf(a.s[q] * __ldg(a.z3 + p * 16 + ax * 5 + q), -bp), bp);
+      Fm[ax][q] = fminf(fmaxf(a.s[q] * __ldg(a.z3 + nb[ax][0] * 16 + ax * 5 + q), -bm), bm);
+    }
+  }
+}
+
+// Write un to the cell unless it breaks positivity (then count the switch-off).
+__device__ __forceinline__ void gated_store(const FixArgs& a, const int c[3], const float un[5]) {
+  const Layout& L = a.lay;
+  const float ke = 0.5f * (un[1] * un[1] + un[2] * un[2] + un[3] * un[3]) / un[0];
+  const float pr = (a.gamma - 1.f) * (un[4] - ke);
+  if (un[0] > 0.f && pr > 0.f && isfinite(pr)) {
+#pragma unroll
+    for (int q = 0; q < 5; ++q) a.uout[L.idx(q, c[2] + 1, c[1] + 1, c[0] + 1)] = un[q];
+  } else if (a.nswitch) {
+    atomicAdd(a.nswitch, 1ull);
+  }
+}
+
 __global__ void __launch_bounds__(256) closure_fix_kernel(const FixArgs a) {
   if (a.clk && !a.clk->active) return;
-  const float dt = a.clk ? (float)a.clk->dt : a.dt_host;
+  const float cdt = a.coef * (a.clk ? (float)a.clk->dt : a.dt_host);
   const Layout& L = a.lay;
   const long long n = (long long)L.nx * L.ny * L.nz;
-  const int dims[3] = {L.nx, L.ny, L.nz};
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
     const int c[3] = {(int)(p % L.nx), (int)((p / L.nx) % L.ny), (int)(p / ((long long)L.nx * L.ny))};
-    float u0[5];
-    load_cell(a, c[0], c[1], c[2], u0);
-    float r[5] = {0, 0, 0, 0, 0};
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
-      int cp[3] = {c[0], c[1], c[2]}, cm[3] = {c[0], c[1], c[2]};
-      cp[ax] = (c[ax] + 1) % dims[ax];
-      cm[ax] = (c[ax] + dims[ax] - 1) % dims[ax];
-      float up[5], um[5];
-      load_cell(a, cp[0], cp[1], cp[2], up);
-      load_cell(a, cm[0], cm[1], cm[2], um);
-      const float s0 = wave_speed(u0, ax, a.gamma);
-      const float sp = fmaxf(s0, wave_speed(up, ax, a.gamma));
-      const float sm = fmaxf(s0, wave_speed(um, ax, a.gamma));
-      const long long pmin = ((long long)cm[2] * L.ny + cm[1]) * L.nx + cm[0];
-#pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        const float bp = a.beta * sp * fabsf(up[q] - u0[q]);
-        const float bm = a.beta * sm * fabsf(u0[q] - um[q]);
-        const float fp = fminf(fmaxf(a.s[q] * __ldg(a.z3 + p * 16 + ax * 5 + q), -bp), bp);
-        const float fm = fminf(fmaxf(a.s[q] * __ldg(a.z3 + pmin * 16 + ax * 5 + q), -bm), bm);
-        r[q] -= (fp - fm) * a.inv_h[ax];
-      }
-    }
+    float Fp[3][5], Fm[3][5];
+    long long nb[3][2];
+    face_corrections(a, c, p, Fp, Fm, nb);
     float un[5];
-    const float cdt = a.coef * dt;
 #pragma unroll
-    for (int q = 0; q < 5; ++q) un[q] = a.uout[L.idx(q, c[2] + 1, c[1] + 1, c[0] + 1)] + cdt * r[q];
-    const float ke = 0.5f * (un[1] * un[1] + un[2] * un[2] + un[3] * un[3]) / un[0];
-    const float pr = (a.gamma - 1.f) * (un[4] - ke);
-    if (un[0] > 0.f && pr > 0.f && isfinite(pr)) {
+    for (int q = 0; q < 5; ++q) {
+      float r = 0.f;
 #pragma unroll
-      for (int q = 0; q < 5; ++q) a.uout[L.idx(q, c[2] + 1, c[1] + 1, c[0] + 1)] = un[q];
-    } else if (a.nswitch) {
-      atomicAdd(a.nswitch, 1ull);
+      for (int ax = 0; ax < 3; ++ax) r -= (Fp[ax][q] - Fm[ax][q]) * a.inv_h[ax];
+      un[q] = a.uout[L.idx(q, c[2] + 1, c[1] + 1, c[0] + 1)] + cdt * r;
     }
+    gated_store(a, c, un);
+  }
+}
+
+// Flux-corrected transport (Zalesak 1979) bound on the corrections: the
+// corrected stage result stays inside [min, max] of the plain stage result
+// (uout before correction) over the cell and its six face neighbours, so the
+// corrections create no new extrema.  Pass 1: per cell and variable the
+// fractions R+ (of the summed inflows) and R- (of the summed outflows) that
+// fit inside those bounds, ratio[q][p] and ratio[5+q][p].
+__global__ void __launch_bounds__(256) fct_ratio_kernel(const FixArgs a) {
+  if (a.clk && !a.clk->active) return;
+  const float cdt = a.coef * (a.clk ? (float)a.clk->dt : a.dt_host);
+  const Layout& L = a.lay;
+  const long long n = (long long)L.nx * L.ny * L.nz;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int c[3] = {(int)(p % L.nx), (int)((p / L.nx) % L.ny), (int)(p / ((long long)L.nx * L.ny))};
+    float Fp[3][5], Fm[3][5];
+    long long nb[3][2];
+    face_corrections(a, c, p, Fp, Fm, nb);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const float ul = a.uout[L.idx(q, c[2] + 1, c[1] + 1, c[0] + 1)];
+      float hi = ul, lo = ul, pin = 0.f, pout = 0.f;
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        // inflow through the +face is -cdt*Fp/h, through the -face +cdt*Fm/h
+        const float tp = -cdt * Fp[ax][q] * a.inv_h[ax], tm = cdt * Fm[ax][q] * a.inv_h[ax];
+        pin += fmaxf(tp, 0.f) + fmaxf(tm, 0.f);
+        pout += fmaxf(-tp, 0.f) + fmaxf(-tm, 0.f);
+#pragma unroll
+        for (int sd = 0; sd < 2; ++sd) {
+          const long long m = nb[ax][sd];
+          const int mi = (int)(m % L.nx), mj = (int)((m / L.nx) % L.ny), mk = (int)(m / ((long long)L.nx * L.ny));
+          const float un = a.uout[L.idx(q, mk + 1, mj + 1, mi + 1)];
+          hi = fmaxf(hi, un);
+          lo = fminf(lo, un);
+        }
+      }
+      a.ratio[(long long)q * n + p] = pin > 0.f ? fminf(1.f, (hi - ul) / pin) : 1.f;
+      a.ratio[(long long)(5 + q) * n + p] = pout > 0.f ? fminf(1.f, (ul - lo) / pout) : 1.f;
+    }
+  }
+}
+
+// Pass 2: each face transfer T (from the lower to the upper cell) is scaled
+// by C = min(R+ of the receiving cell, R- of the giving cell), the same factor
+// seen from both cells, so the limited correction stays conservative.
+__global__ void __launch_bounds__(256) fct_apply_kernel(const FixArgs a) {
+  if (a.clk && !a.clk->active) return;
+  const float cdt = a.coef * (a.clk ? (float)a.clk->dt : a.dt_host);
+  const Layout& L = a.lay;
+  const long long n = (long long)L.nx * L.ny * L.nz;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int c[3] = {(int)(p % L.nx), (int)((p / L.nx) % L.ny), (int)(p / ((long long)L.nx * L.ny))};
+    float Fp[3][5], Fm[3][5];
+    long long nb[3][2];
+    face_corrections(a, c, p, Fp, Fm, nb);
+    float un[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const float* Rp = a.ratio + (long long)q * n;        // R+
+      const float* Rm = a.ratio + (long long)(5 + q) * n;  // R-
+      const float rp0 = Rp[p], rm0 = Rm[p];
+      float d = 0.f;
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        // +face: transfer T from this cell to the one above
+        const float T = cdt * Fp[ax][q] * a.inv_h[ax];
+        const long long up = nb[ax][1], dn = nb[ax][0];
+        const float Cp = T >= 0.f ? fminf(Rp[up], rm0) : fminf(rp0, Rm[up]);
+        // -face: transfer T' from the cell below to this one
+        const float Tm = cdt * Fm[ax][q] * a.inv_h[ax];
+        const float Cm = Tm >= 0.f ? fminf(rp0, Rm[dn]) : fminf(Rp[dn], rm0);
+        d += Cm * Tm - Cp * T;
+      }
+      un[q] = a.uout[L.idx(q, c[2] + 1, c[1] + 1, c[0] + 1)] + d;
+    }
+    gated_store(a, c, un);
   }
 }
 

@@ -145,24 +145,48 @@ def box_filter(U, f):
     return U.reshape(nv, a // f, f, b // f, f, c // f, f).mean(axis=(2, 4, 6))
 
 
-def correct(uin, uout, Z3, s, beta, gamma, coef, dt, h):
+def correct(uin, uout, Z3, s, beta, gamma, coef, dt, h, fct=False):
     """Per-stage correction: face flux corrections s_q Z3 clipped to
     +-beta * max(|v_a| + c) * |U_q(p + e_a) - U_q(p)| (taken from the stage
     input uin), their divergence added to uout with weight coef*dt, and cells
-    whose result has rho <= 0 or p <= 0 left at uout.  Returns (new, count)."""
+    whose result has rho <= 0 or p <= 0 left at uout.  With ``fct`` the face
+    transfers are first limited by flux-corrected transport (Zalesak 1979):
+    the result stays within the min/max of uout over each cell and its six
+    face neighbours.  Returns (new, count)."""
     uin = np.asarray(uin, np.float64)
     rho, v, p = primitives(uin, gamma)
     c = np.where((p > 0) & (rho > 0), np.sqrt(np.abs(gamma * p / rho)), 0.0)
-    R = np.zeros_like(uin)
+    T = np.zeros((3,) + uin.shape)  # transfer through the +x_a face, from the cell to its upper neighbour
     for a in range(3):
         ax = _axis(a)
         sp = np.abs(v[a]) + c
         smax = np.maximum(sp, np.roll(sp, -1, axis=ax))
         for q in range(5):
             bound = beta * smax * np.abs(np.roll(uin[q], -1, axis=ax) - uin[q])
-            F = np.clip(s[q] * Z3[..., a * 5 + q], -bound, bound)
-            R[q] -= (F - np.roll(F, 1, axis=ax)) / h[a]
-    un = uout + coef * dt * R
+            T[a, q] = coef * dt * np.clip(s[q] * Z3[..., a * 5 + q], -bound, bound) / h[a]
+    if fct:
+        hi, lo = uout.copy(), uout.copy()
+        pin, pout = np.zeros_like(uout), np.zeros_like(uout)
+        for a in range(3):
+            ax = _axis(a)
+            for sh in (1, -1):
+                nbv = np.roll(uout, sh, axis=ax + 1)
+                hi, lo = np.maximum(hi, nbv), np.minimum(lo, nbv)
+            tin = [-T[a], np.roll(T[a], 1, axis=ax + 1)]  # inflow through the +face and the -face
+            for t in tin:
+                pin += np.maximum(t, 0.0)
+                pout += np.maximum(-t, 0.0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            Rp = np.where(pin > 0, np.minimum(1.0, (hi - uout) / pin), 1.0)
+            Rm = np.where(pout > 0, np.minimum(1.0, (uout - lo) / pout), 1.0)
+        for a in range(3):
+            ax = _axis(a) + 1
+            Rp_up, Rm_up = np.roll(Rp, -1, axis=ax), np.roll(Rm, -1, axis=ax)
+            T[a] *= np.where(T[a] >= 0, np.minimum(Rp_up, Rm), np.minimum(Rp, Rm_up))
+    R = np.zeros_like(uin)
+    for a in range(3):
+        R -= T[a] - np.roll(T[a], 1, axis=_axis(a) + 1)
+    un = uout + R
     ke = 0.5 * (un[1] ** 2 + un[2] ** 2 + un[3] ** 2) / un[0]
     pr = (gamma - 1.0) * (un[4] - ke)
     ok = (un[0] > 0) & (pr > 0) & np.isfinite(pr)

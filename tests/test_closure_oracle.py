@@ -123,3 +123,22 @@ def test_bf16_rounding_is_nearest_even():
     r = co.bf16(x)
     assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6 and r[3] == -1.5
     assert abs(r[4] - 3.14159) < 2 ** -7 * 4
+
+
+def test_fct_correction_creates_no_new_extrema_and_conserves():
+    rng = np.random.default_rng(6)
+    n = (4, 6, 8)
+    rho = rng.uniform(1.0, 2.0, n)
+    v = rng.normal(0, 0.3, (3,) + n)
+    p = rng.uniform(2, 3, n)
+    u = np.stack([rho, rho * v[0], rho * v[1], rho * v[2], p / 0.4 + 0.5 * rho * (v * v).sum(0)])
+    Z3 = rng.normal(0, 1, n + (16,))
+    big, nsw = co.correct(u, u.copy(), Z3, np.ones(5), 1e3, 1.4, 1.0, 1e-2, (0.1, 0.1, 0.1), fct=True)
+    hi, lo = u.copy(), u.copy()
+    for ax in (1, 2, 3):
+        for sh in (1, -1):
+            hi, lo = np.maximum(hi, np.roll(u, sh, axis=ax)), np.minimum(lo, np.roll(u, sh, axis=ax))
+    assert nsw == 0
+    assert np.all(big <= hi + 1e-12) and np.all(big >= lo - 1e-12)
+    assert np.allclose(big.sum(axis=(1, 2, 3)), u.sum(axis=(1, 2, 3)), rtol=1e-12)
+    assert np.max(np.abs(big - u)) > 1e-3  # the limited correction still acts

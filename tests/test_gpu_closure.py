@@ -177,11 +177,13 @@ def test_filter_and_dense_copies():
         _close(ours, co.box_filter(u.astype(np.float64), f), f"filter {f}", rel=1e-7)
 
 
-def test_correct_dense_matches_oracle():
+@pytest.mark.parametrize("fct", [False, True], ids=["clip", "fct"])
+def test_correct_dense_matches_oracle(fct):
     import torch
     n = (32, 32, 16)
     rng = np.random.default_rng(5)
     c = _closure(n, out_scale=np.full(5, 0.2))
+    c.set_limiter(fct)
     c.set_weights(_rand_params(rng, scale=2.0))
     uin = _random_state((n[2], n[1], n[0]), rng)
     uout = (uin * (1 + 1e-3 * rng.standard_normal(uin.shape))).astype(np.float32)
@@ -192,7 +194,8 @@ def test_correct_dense_matches_oracle():
     for beta, dt, coef in ((0.5, 1e-3, 1.0), (0.5, 1e-3, 0.25), (50.0, 5.0, 1.0)):
         out = torch.from_numpy(uout.copy()).cuda()
         nsw = c.correct_dense(torch.from_numpy(uin).cuda(), out, coef, dt, beta, h)
-        ref, nref = co.correct(uin, uout.astype(np.float64), Z3, c.norm["out_scale"], beta, GAMMA, coef, dt, h)
+        ref, nref = co.correct(uin, uout.astype(np.float64), Z3, c.norm["out_scale"], beta, GAMMA, coef, dt, h,
+                               fct=fct)
         ours = out.cpu().numpy()
         if nref == 0:
             assert nsw == 0
@@ -204,13 +207,15 @@ def test_correct_dense_matches_oracle():
             assert np.all(rho > 0) and np.all(p > 0)
 
 
-def test_attached_euler_step_is_plain_step_plus_correction():
+@pytest.mark.parametrize("fct", [False, True], ids=["clip", "fct"])
+def test_attached_euler_step_is_plain_step_plus_correction(fct):
     import torch
     from multiphysics_fvm_b200 import closure as CL
     from multiphysics_fvm_b200.numerics import time_integrators as ti
     n = (32, 32, 16)
     rng = np.random.default_rng(6)
     c = _closure(n, out_scale=np.full(5, 0.02))
+    c.set_limiter(fct)
     c.set_weights(_rand_params(rng))
     _, sim = _kh_sim(n, ti.euler_explicit)
     _, ref = _kh_sim(n, ti.euler_explicit)
