@@ -150,6 +150,18 @@ int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_ker
  * the state and clock are restored afterwards.  New: the reference has no tuning. */
 int fvm_autotune(fvm_handle* h, int* best_zchunk, double* best_ms_per_step);
 
+/* Sharp Kelvin-Helmholtz initial state written on the device (the host
+ * initializer of setups/kelvin_helmholtz_sharp.py, done in HBM instead of on
+ * the host and uploaded; replaces solver.apply_ics, src/solver.py:64-85, for
+ * this setup).  params: {rho_inner, rho_outer, shear_velocity, pressure,
+ * amplitude, wavenumber, noise, phase, noise_all}: rho and v1 = +-shear inside /
+ * outside |x2 - 0.5| < 0.25, v2 = amplitude*sin(2 pi wavenumber x1 + phase) +
+ * noise, v1 and v3 get noise too when noise_all != 0, P = pressure, gamma from
+ * the descriptor.  Noise is uniform in [-noise, noise) from a counter-based hash
+ * of (seed, variable, cell), so it is reproducible for any grid but is not
+ * NumPy's draw.  navier_stokes handles only; ghosts are filled by the step. */
+int fvm_init_kelvin_helmholtz(fvm_handle* h, const double params[9], unsigned long long seed);
+
 /* ---- batches of independent grids (SURVEY configuration C3) -------------------
  * Many setups of uneven sizes advance together: one persistent launch per kernel
  * specialisation and stage walks a flat tile list over all grids, and every grid

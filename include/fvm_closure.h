@@ -84,6 +84,13 @@ int fvm_closure_adam(fvm_closure* c, double lr, double beta1, double beta2, doub
 /* features + forward + backward + adam. */
 int fvm_closure_train_step(fvm_closure* c, const float* u_dense_dev, const float* defect_dense_dev, double dt,
                            const double h[3], double lr);
+/* Device time per call (CUDA events on the closure's stream, one untimed
+ * warm-up, `iters` back-to-back calls): the forward pass from the current
+ * features, and the full training step (features, forward, loss, backward,
+ * Adam -- the weights change). */
+int fvm_closure_time_forward(fvm_closure* c, int iters, double* ms);
+int fvm_closure_time_train(fvm_closure* c, const float* u_dense_dev, const float* defect_dense_dev, double dt,
+                           const double h[3], double lr, int iters, double* ms);
 /* Loss of the last backward (synchronises). */
 int fvm_closure_loss(fvm_closure* c, double* out);
 

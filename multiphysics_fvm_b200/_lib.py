@@ -74,6 +74,7 @@ SIGNATURES = [
     ("fvm_batch_step", C.c_int, [_P, C.c_int, C.c_int]),
     ("fvm_batch_time_steps", C.c_int, [_P, C.c_int, C.c_int, _DP]),
     ("fvm_batch_autotune", C.c_int, [_P, C.POINTER(C.c_int), _DP]),
+    ("fvm_init_kelvin_helmholtz", C.c_int, [_P, _DP, C.c_ulonglong]),
     # learned closure (include/fvm_closure.h)
     ("fvm_closure_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(_P)]),
     ("fvm_closure_destroy", C.c_int, [_P]),
@@ -89,6 +90,8 @@ SIGNATURES = [
     ("fvm_closure_adam", C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_double]),
     ("fvm_closure_train_step", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_double, _DP, C.c_double]),
     ("fvm_closure_loss", C.c_int, [_P, _DP]),
+    ("fvm_closure_time_forward", C.c_int, [_P, C.c_int, _DP]),
+    ("fvm_closure_time_train", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_double, _DP, C.c_double, C.c_int, _DP]),
     ("fvm_closure_correct_dense", C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double, _DP,
                                             C.POINTER(C.c_ulonglong)]),
     ("fvm_closure_attach", C.c_int, [_P, _P, C.c_double]),

@@ -204,6 +204,15 @@ class Simulation:
         for q, k in enumerate(self.variables):
             U[k][...] = arr[q]
 
+    def init_kelvin_helmholtz(self, ics: dict, seed: int):
+        """Write the sharp Kelvin-Helmholtz state of setups/kelvin_helmholtz_sharp
+        on the device (``ics`` = its initial_conditions parameters); the noise is
+        a counter-based draw, not NumPy's."""
+        keys = ("rho_inner", "rho_outer", "shear_velocity", "pressure", "amplitude", "wavenumber", "noise", "phase")
+        prm = np.array([float(ics.get(k, 0.0)) for k in keys] + [1.0 if ics.get("noise_all") else 0.0])
+        L.check(self._lib.fvm_init_kelvin_helmholtz(self._h, L.dptr(prm), C.c_ulonglong(int(seed))),
+                "fvm_init_kelvin_helmholtz")
+
     # -- hot path ------------------------------------------------------------
     def residual(self) -> np.ndarray:
         out = np.empty((self.nv,) + self.n, dtype=np.float64)

@@ -179,6 +179,21 @@ class Closure:
                                                  _dev_ptr(defect, self.dense_shape), float(dt), L.dptr(hh),
                                                  float(lr)), "fvm_closure_train_step")
 
+    def time_forward(self, iters: int = 20) -> float:
+        """Device ms per forward pass (from the current features)."""
+        v = C.c_double()
+        L.check(self._lib.fvm_closure_time_forward(self._h, int(iters), C.byref(v)), "fvm_closure_time_forward")
+        return v.value
+
+    def time_train(self, u, defect, dt: float, h, lr: float = 1e-3, iters: int = 20) -> float:
+        """Device ms per full training step (the weights change)."""
+        hh = np.ascontiguousarray(h, dtype=np.float64)
+        v = C.c_double()
+        L.check(self._lib.fvm_closure_time_train(self._h, _dev_ptr(u, self.dense_shape),
+                                                 _dev_ptr(defect, self.dense_shape), float(dt), L.dptr(hh),
+                                                 float(lr), int(iters), C.byref(v)), "fvm_closure_time_train")
+        return v.value
+
     def loss(self) -> float:
         v = C.c_double()
         L.check(self._lib.fvm_closure_loss(self._h, C.byref(v)), "fvm_closure_loss")

@@ -60,10 +60,14 @@ def kh_setup(n: int, seed: int):
     return kh.get_setup(n, n, n, seed=seed, precision="fp32", noise_all=True)
 
 
-def new_sim(n: int, seed: int, initial_state: bool = True):
+def new_sim(n: int, seed: int, initial_state: bool = True, device_ic: bool = True):
+    """A float32 3D KH simulation; the initial state is written on the device
+    (counter-based noise) or by the host initializer (NumPy noise) and uploaded."""
     s = kh_setup(n, seed)
     sim = backend.Simulation.from_setup(s)
-    if initial_state:
+    if initial_state and device_ic:
+        sim.init_kelvin_helmholtz(s["initial_conditions"]["parameters"], seed)
+    elif initial_state:
         g = build_grid(s["coordinate_system"], s["grid_config"])
         U = s["physics"].allocate_u(s["grid_config"])
         s["initial_conditions"]["initializer"](U, s["physical_parameters"], g, s["initial_conditions"]["parameters"])
@@ -79,26 +83,24 @@ def generate(cfg: Config, seeds, log=print):
     window and keeps the persistent part that a correction can carry."""
     import torch
     f, nc, k = cfg.factor, cfg.coarse, cfg.defect_steps
-    if k > cfg.sample_every:
-        raise ValueError("defect_steps must not exceed sample_every")
     coarse = new_sim(nc, 0, initial_state=False)
     Us, Ds = [], []
     for seed in seeds:
         t0 = time.time()
         fine = new_sim(cfg.fine, seed)
-        pending = None
+        pending = []  # (coarse step at which the window ends, filtered start state)
         for m in range(cfg.n_coarse_steps + 1):
-            if pending is not None and m == pending[0]:
+            if pending and m == pending[0][0]:
+                _, ub0 = pending.pop(0)
                 ubk = CL.filter_state(fine, f)
-                CL.upload_dense(coarse, pending[1])
+                CL.upload_dense(coarse, ub0)
                 coarse.step(k, dt=cfg.dt_coarse)
                 Ds.append((ubk - CL.download_dense(coarse)) / k)
-                Us.append(pending[1])
-                pending = None
+                Us.append(ub0)
             if m == cfg.n_coarse_steps:
                 break
             if m % cfg.sample_every == 0 and m + k <= cfg.n_coarse_steps:
-                pending = (m + k, CL.filter_state(fine, f))
+                pending.append((m + k, CL.filter_state(fine, f)))
             fine.step(f, dt=cfg.dt_coarse / f)
         st = fine.status()
         fine.close()

@@ -283,6 +283,28 @@ int sync_status(fvm_closure* c) {
   return FVM_OK;
 }
 
+// Device time (CUDA events on the closure's stream) of `iters` back-to-back
+// launches of work, after one untimed warm-up.
+template <class F>
+int time_on_stream(fvm_closure* c, int iters, double* ms, F work) {
+  if (!ms || iters < 1) return set_error(FVM_E_INVALID, "closure timing: iters >= 1 and a result pointer");
+  cudaEvent_t a = nullptr, b = nullptr;
+  CL_CK(cudaEventCreate(&a));
+  CL_CK(cudaEventCreate(&b));
+  cudaError_t e = work();
+  if (e == cudaSuccess) e = cudaEventRecord(a, c->stream);
+  for (int i = 0; i < iters && e == cudaSuccess; ++i) e = work();
+  if (e == cudaSuccess) e = cudaEventRecord(b, c->stream);
+  if (e == cudaSuccess) e = cudaEventSynchronize(b);
+  float t = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e != cudaSuccess) return set_error(FVM_E_CUDA, std::string("closure timing: ") + cudaGetErrorString(e));
+  *ms = t / iters;
+  return sync_status(c);
+}
+
 }  // namespace
 
 namespace fvm {
@@ -329,7 +351,9 @@ int fvm_closure_create(int n1, int n2, int n3, unsigned long long seed, fvm_clos
   c->n3 = n3;
   c->npos = (long long)n1 * n2 * n3;
   cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
-  c->zc_conv = largest_zc(n3, (long long)(n1 / 8) * (n2 / 16), 2ll * c->nsm);
+  // conv CTAs are serial load -> MMA -> epilogue chains: aim for about four
+  // resident per SM (shared memory allows 3-4) so their waits overlap
+  c->zc_conv = largest_zc(n3, (long long)(n1 / 8) * (n2 / 16), 4ll * c->nsm);
   c->zc_wg = largest_zc(n3, (long long)(n1 / 16) * (n2 / 8), 2ll * c->nsm);
   const long long wg_blocks = (long long)(n1 / 16) * (n2 / 8) * (n3 / c->zc_wg);
   c->partial_elems = (size_t)wg_blocks * 27 * C_HID * C_HID + (size_t)2 * c->nsm * C_HID;
@@ -532,6 +556,26 @@ int fvm_closure_train_step(fvm_closure* c, const float* u_dense_dev, const float
   CL_CK(adam_all(c, true, (float)lr, 0.9f, 0.999f, 1e-8f, c->stream));
   // inputs belong to the caller: finish with them before returning
   return sync_status(c);
+}
+
+int fvm_closure_time_forward(fvm_closure* c, int iters, double* ms) {
+  if (int rc = check(c)) return rc;
+  return time_on_stream(c, iters, ms, [&]() { return forward(c, c->stream); });
+}
+
+int fvm_closure_time_train(fvm_closure* c, const float* u_dense_dev, const float* defect_dense_dev, double dt,
+                           const double h[3], double lr, int iters, double* ms) {
+  if (int rc = check(c)) return rc;
+  if (!u_dense_dev || !defect_dense_dev || !h || !(h[0] > 0 && h[1] > 0 && h[2] > 0))
+    return set_error(FVM_E_INVALID, "closure timing: bad arguments");
+  const Layout L = dense_layout(c->n1, c->n2, c->n3);
+  return time_on_stream(c, iters, ms, [&]() {
+    cudaError_t e = features(c, u_dense_dev, L, c->gamma, c->stream);
+    if (e == cudaSuccess) e = forward(c, c->stream);
+    if (e == cudaSuccess) e = backward(c, defect_dense_dev, dt, h, c->stream);
+    if (e == cudaSuccess) e = adam_all(c, true, (float)lr, 0.9f, 0.999f, 1e-8f, c->stream);
+    return e;
+  });
 }
 
 int fvm_closure_loss(fvm_closure* c, double* out) {

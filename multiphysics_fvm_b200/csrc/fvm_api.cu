@@ -1402,3 +1402,31 @@ int fvm_upload_dense(fvm_handle* h, const float* dense_dev) { return dense_copy(
 int fvm_download_dense(fvm_handle* h, float* dense_dev) { return dense_copy(h, dense_dev, 0); }
 
 }  // extern "C"
+
+// ------------------------------------------------------ device initial state ----
+extern "C" int fvm_init_kelvin_helmholtz(fvm_handle* h, const double params[9], unsigned long long seed) {
+  if (!h || !params) return fail(FVM_E_INVALID, "null argument");
+  if (h->d.physics != FVM_NAVIER_STOKES) return fail(FVM_E_INVALID, "Kelvin-Helmholtz state: navier_stokes only");
+  KhInit k{};
+  k.rho_in = params[0];
+  k.rho_out = params[1];
+  k.shear = params[2];
+  k.pres = params[3];
+  k.amp = params[4];
+  k.wavenumber = params[5];
+  k.noise = params[6];
+  k.phase = params[7];
+  k.noise_all = params[8] != 0.0;
+  k.gamma = h->d.params[0];
+  k.x1_min = h->d.x1_min;
+  k.dx1 = (h->d.x1_max - h->d.x1_min) / h->d.nx1;
+  k.x2_min = h->d.x2_min;
+  k.dx2 = (h->d.x2_max - h->d.x2_min) / h->d.nx2;
+  k.seed = seed;
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  if (h->f64) kh_init_kernel<double><<<4 * h->nsm, 256, 0, h->stream>>>(static_cast<double*>(h->U[0]), h->lay, k);
+  else kh_init_kernel<float><<<4 * h->nsm, 256, 0, h->stream>>>(static_cast<float*>(h->U[0]), h->lay, k);
+  FVM_CK(cudaGetLastError());
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}

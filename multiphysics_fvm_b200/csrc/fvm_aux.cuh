@@ -285,4 +285,47 @@ __global__ void totals_final_kernel(const double* __restrict__ partials, int nbl
   out[threadIdx.x] = s + c;
 }
 
+// ------------------------------------------------------ device initial state ----
+// Uniform value in [-1, 1) from a splitmix64 hash of (seed, stream, index).
+__device__ __forceinline__ double hash_unit(unsigned long long seed, unsigned long long stream, long long i) {
+  unsigned long long z = seed * 0x9E3779B97F4A7C15ull + (stream + 1) * 0xD1B54A32D192ED03ull + (unsigned long long)i;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+struct KhInit {
+  double rho_in, rho_out, shear, pres, amp, wavenumber, noise, phase, gamma;
+  double x1_min, dx1, x2_min, dx2;
+  int noise_all;
+  unsigned long long seed;
+};
+
+// Sharp Kelvin-Helmholtz state (float64 arithmetic, stored in Real) on the
+// interior of buffer u.
+template <typename Real>
+__global__ void kh_init_kernel(Real* u, Layout L, KhInit k) {
+  const long long n = (long long)L.nx * L.ny * L.nz;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(p % L.nx), j = (int)((p / L.nx) % L.ny), kk = (int)(p / ((long long)L.nx * L.ny));
+    const double x = k.x1_min + (i + 0.5) * k.dx1, y = k.x2_min + (j + 0.5) * k.dx2;
+    const bool inner = fabs(y - 0.5) < 0.25;
+    const double rho = inner ? k.rho_in : k.rho_out;
+    double v1 = inner ? k.shear : -k.shear;
+    double v2 = k.amp * sin(2.0 * 3.141592653589793 * k.wavenumber * x + k.phase) + k.noise * hash_unit(k.seed, 1, p);
+    double v3 = 0.0;
+    if (k.noise_all) {
+      v1 += k.noise * hash_unit(k.seed, 0, p);
+      v3 += k.noise * hash_unit(k.seed, 2, p);
+    }
+    const double e = k.pres / (k.gamma - 1.0) + 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3);
+    u[L.idx(0, kk + 1, j + 1, i + 1)] = (Real)rho;
+    u[L.idx(1, kk + 1, j + 1, i + 1)] = (Real)(rho * v1);
+    u[L.idx(2, kk + 1, j + 1, i + 1)] = (Real)(rho * v2);
+    u[L.idx(3, kk + 1, j + 1, i + 1)] = (Real)(rho * v3);
+    u[L.idx(4, kk + 1, j + 1, i + 1)] = (Real)e;
+  }
+}
+
 }  // namespace fvm

@@ -206,7 +206,7 @@ template <typename Real, int LIM, int RIEM, int COORD>
 cudaError_t launch_maxwell_one(const CUtensorMap& map, MaxwellParams<Real> p, cudaStream_t s, int nsm) {
   constexpr int TY = maxwell_tile_ty<Real>();
   using C = MaxwellCfg<Real, TY>;
-  auto kern = maxwell_stage_kernel<Real, LIM, RIEM, COORD, TY, std::is_same<Real, double>::value ? 1 : 2>;
+  auto kern = maxwell_stage_kernel<Real, LIM, RIEM, COORD, TY, std::is_same<Real, double>::value ? 1 : 3>;
   static int bps = 0;
   if (bps == 0 || nsm < 0) {
     cudaError_t e = prepare_kernel(kern, C::NT, C::BYTES, &bps);
