@@ -296,15 +296,19 @@ __global__ void __launch_bounds__(128, 1) conv3_kernel(const ConvArgs a) {
       if (tid == 0) {
         tc_fence_after();
         const uint32_t dcol = tbase + (uint32_t)((i & 1) * COUT);
-#pragma unroll 1
+        // A tap shift only moves the 14-bit start-address field, so every
+        // descriptor is a per-step base plus a compile-time constant (the
+        // addresses stay below 256 KB: no carry out of the field).
+        uint64_t abase[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) abase[d] = sdesc(sbase + C::OFF_RING + ((i + d) & 3) * C::PLANEB, C::CHB, C::ROWB);
+        const uint64_t bbase = sdesc(sbase + C::OFF_W, COUT * 16, 128);
+#pragma unroll
         for (int t = 0; t < 27; ++t) {
-          const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-          const uint32_t aslot = sbase + C::OFF_RING + ((i + dz + 1) & 3) * C::PLANEB;
 #pragma unroll
           for (int s = 0; s < C::KS; ++s) {
-            const uint64_t ad =
-                sdesc(aslot + (dy + 1) * C::ROWB + 2 * s * C::CHB + (dx + 1) * 16, C::CHB, C::ROWB);
-            const uint64_t bd = sdesc(sbase + C::OFF_W + (t * C::KS + s) * 2 * COUT * 16, COUT * 16, 128);
+            const uint64_t ad = abase[t / 9] + (uint64_t)(((t / 3) % 3 * C::ROWB + 2 * s * C::CHB + (t % 3) * 16) >> 4);
+            const uint64_t bd = bbase + (uint64_t)(((t * C::KS + s) * 2 * COUT * 16) >> 4);
             umma_bf16(dcol, ad, bd, IDESC, (t | s) != 0 ? 1u : 0u);
           }
         }
@@ -472,17 +476,21 @@ __global__ void __launch_bounds__(128, 1) wgrad_kernel(const WgradArgs a) {
     if (!aborted) {
       if (tid == 0) {
         tc_fence_after();
-        const uint32_t gslot = sbase + C::OFF_G + (i & 1) * C::GPLANEB;
-#pragma unroll 1
+        // descriptors = per-step bases + compile-time offsets (see conv3_kernel)
+        const uint64_t bbase = sdesc(sbase + C::OFF_G + (i & 1) * C::GPLANEB, 128, C::GCHB);
+        uint64_t abase[3];
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz) abase[dz] = sdesc(sbase + C::OFF_X + ((i + dz) & 3) * C::PLANEB, 128, C::CHB);
+        const uint32_t acc0 = i != 0 ? 1u : 0u;
+#pragma unroll
         for (int yl = 0; yl < C::TY; ++yl) {
-          const uint64_t bd = sdesc(gslot + yl * C::GROWB, 128, C::GCHB);
+          const uint64_t bd = bbase + (uint64_t)((yl * C::GROWB) >> 4);
 #pragma unroll
           for (int dz = 0; dz < 3; ++dz) {
-            const uint32_t xrow = sbase + C::OFF_X + ((i + dz) & 3) * C::PLANEB + yl * C::ROWB;
 #pragma unroll
             for (int dx = 0; dx < 3; ++dx) {
-              const uint64_t ad = sdesc(xrow + dx * 16, 128, C::CHB);
-              umma_bf16(tbase + (uint32_t)((dz * 3 + dx) * COUT), ad, bd, IDESC, (i | yl) != 0 ? 1u : 0u);
+              const uint64_t ad = abase[dz] + (uint64_t)((yl * C::ROWB + dx * 16) >> 4);
+              umma_bf16(tbase + (uint32_t)((dz * 3 + dx) * COUT), ad, bd, IDESC, yl != 0 ? 1u : acc0);
             }
           }
         }
