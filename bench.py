@@ -25,6 +25,7 @@ import json
 import math
 import os
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -85,7 +86,7 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"fvm_bench_clocks_rank{gpu_index}_{os.getpid()}.csv")
 
     def __enter__(self):
         try:

@@ -162,7 +162,7 @@ int fvm_autotune(fvm_handle* h, int* best_zchunk, double* best_ms_per_step);
  * NumPy's draw.  navier_stokes handles only; ghosts are filled by the step. */
 int fvm_init_kelvin_helmholtz(fvm_handle* h, const double params[9], unsigned long long seed);
 
-/* ---- batches of independent grids (SURVEY configuration C3) -------------------
+/* ---- batches of independent grids ----------------------------------------------
  * Many setups of uneven sizes advance together: one persistent launch per kernel
  * specialisation and stage walks a flat tile list over all grids, and every grid
  * keeps its own CFL time step.  All grids share the time integrator and the
