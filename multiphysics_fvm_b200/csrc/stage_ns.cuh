@@ -445,10 +445,15 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       if (K < Z0) { __syncthreads(); continue; }
       const int kK = K - 1;  // interior index of the output plane
       // ------------------------------------------------ G: x1 slopes ----
+      // Task maps of the x1 phases: warp w < TY takes the 32 cells (faces) of
+      // row w, the two spare warps the row ends, so no warp straddles two ring
+      // rows (whose 40-float stride would put lanes on the same bank).
       {
         constexpr int ti[3] = {0, 3, 4};  // tau row 1 = (t11, t12, t13)
-        for (int it = tid; it < TY * (TX + 2); it += NT) {
-          const int ty = it / (TX + 2), tx = it % (TX + 2) - 1;
+        const int hh = tid - TX * TY;     // halo task of a spare-warp thread
+        if (is_out || hh < 2 * TY) {
+          const int ty = is_out ? oty : hh >> 1, tx = is_out ? otx : ((hh & 1) ? TX : -1);
+          const int it = ty * (TX + 2) + tx + 1;
           const int i = x0 + tx, j = y0 + ty;
           const bool interior = i >= 0 && i < nx && j < ny;
           const Real l1 = (F32 || !interior) ? Real(1) : G::L1(p.met, i, j, kK);
@@ -464,8 +469,10 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       __syncthreads();
       {
         constexpr int ti[3] = {0, 3, 4};
-        for (int it = tid; it < TY * (TX + 1); it += NT) {
-          const int ty = it / (TX + 1), fx = it % (TX + 1);
+        const int hh = tid - TX * TY;
+        if (is_out || hh < TY) {
+          const int ty = is_out ? oty : hh, fx = is_out ? otx : TX;
+          const int it = ty * (TX + 1) + fx;
           const int fi = x0 + fx, j = y0 + ty;
           Real F[5] = {Real(0), Real(0), Real(0), Real(0), Real(0)};
           if (fi <= nx && j < ny) {
@@ -497,7 +504,9 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       // ------------------------------------------------ G: x2 slopes ----
       {
         constexpr int ti[3] = {3, 1, 5};  // tau row 2 = (t12, t22, t23)
-        for (int it = tid; it < (TY + 2) * TX; it += NT) {
+        static_assert((TY + 2) * TX == NT, "one x2-slope task per thread");
+        {
+          const int it = tid;
           const int ty = it / TX - 1, tx = it % TX;
           const int i = x0 + tx, j = y0 + ty;
           const bool interior = i < nx && j >= 0 && j < ny;
@@ -514,7 +523,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       __syncthreads();
       {
         constexpr int ti[3] = {3, 1, 5};
-        for (int it = tid; it < (TY + 1) * TX; it += NT) {
+        if (tid < (TY + 1) * TX) {
+          const int it = tid;
           const int fy = it / TX, tx = it % TX;
           const int fj = y0 + fy, i = x0 + tx;
           Real F[5] = {Real(0), Real(0), Real(0), Real(0), Real(0)};
