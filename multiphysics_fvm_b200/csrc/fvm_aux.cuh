@@ -17,13 +17,15 @@ __host__ __device__ inline long long bc_face_count(const Layout& L, int nv) {
 }
 
 // Fill ghost element t (0 <= t < bc_face_count) of one grid.
-template <typename Real>
-__device__ __forceinline__ void bc_fill_one(Real* __restrict__ u, const Layout& L, const BcSpec& bc, long long t) {
-  const long long nyz = (long long)L.ny * L.nz, nxz = (long long)L.nx * L.nz, nxy = (long long)L.nx * L.ny;
-  const long long per_var = 2 * (nyz + nxz + nxy);
+// Idx: the integer type of the element decomposition (32-bit whenever the
+// ghost count fits, which avoids emulated 64-bit division).
+template <typename Real, typename Idx = long long>
+__device__ __forceinline__ void bc_fill_one(Real* __restrict__ u, const Layout& L, const BcSpec& bc, Idx t) {
+  const Idx nyz = (Idx)L.ny * L.nz, nxz = (Idx)L.nx * L.nz, nxy = (Idx)L.nx * L.ny;
+  const Idx per_var = 2 * (nyz + nxz + nxy);
   {
     const int q = (int)(t / per_var);
-    long long r = t % per_var;
+    Idx r = t % per_var;
     int side, a, b;  // a, b: transverse interior indices (0-based)
     if (r < 2 * nyz) { side = r < nyz ? 0 : 1; r %= nyz; a = (int)(r % L.ny); b = (int)(r / L.ny); }
     else if ((r -= 2 * nyz) < 2 * nxz) { side = r < nxz ? 2 : 3; r %= nxz; a = (int)(r % L.nx); b = (int)(r / L.nx); }
@@ -51,9 +53,14 @@ template <typename Real>
 __global__ void bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc, const int* active) {
   if (active && !*active) return;
   const long long total = bc_face_count(L, nv);
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x)
-    bc_fill_one(u, L, bc, t);
+  if (total < 0x7fffffffll) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < (int)total; t += gridDim.x * blockDim.x)
+      bc_fill_one<Real, int>(u, L, bc, t);
+  } else {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x)
+      bc_fill_one<Real, long long>(u, L, bc, t);
+  }
 }
 
 // Reference layout (C order, last axis fastest) <-> device layout (x1 fastest).
@@ -157,10 +164,14 @@ __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, co
   __shared__ double s_rc[32], s_nu[32];
   double rc = 0.0, nu = 0.0;
   unsigned bad = 0;
-  const long long n = (long long)L.nx * L.ny * L.nz;
-  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(c % L.nx), j = (int)((c / L.nx) % L.ny), k = (int)(c / ((long long)L.nx * L.ny));
-    const long long g = L.idx(0, k + 1, j + 1, i + 1);
+  // one x1 row per block iteration, threads across the row: no 64-bit
+  // division per cell (rows = ny*nz < 2^31)
+  const int rows = L.ny * L.nz;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int j = row % L.ny, k = row / L.ny;
+    const long long g0 = L.idx(0, k + 1, j + 1, 1);
+   for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
+    const long long g = g0 + i;
     const double rho = double(u[g]);
     const double v0 = double(u[g + L.var_stride]) / rho, v1 = double(u[g + 2 * L.var_stride]) / rho,
                  v2 = double(u[g + 3 * L.var_stride]) / rho;
@@ -180,6 +191,7 @@ __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, co
     if (!(r >= 0.0) || !(nl >= 0.0)) bad |= ST_NONFINITE;
     rc = fmax(rc, r);
     nu = fmax(nu, nl);
+   }
   }
   for (int o = 16; o > 0; o >>= 1) {
     rc = fmax(rc, __shfl_xor_sync(0xffffffffu, rc, o));

@@ -313,27 +313,30 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         }
       }
       // ---------------------------------------------------------- C ----
-      // P on plane K+2, tile + 2 (navier_stokes.py:94-100)
-      {
-        Real* pw = pring + pmod(flat ? K : K + 2, 3) * PL2;
-        const Real* usrc = flat ? uK : uK2;
-        for (int it = tid; it < C::PL2; it += NT) {
-          const int r2 = it / W2, c2 = it % W2;
-          const Real* u = usrc + (r2 + HH - 2) * W + c2 + 2;
-          const Real rho = u[0];
-          Real v0, v1, v2, E;
-          if constexpr (F32) {
-            const Real ir = rcp_approx(rho);
-            v0 = u[PL] * ir; v1 = u[2 * PL] * ir; v2 = u[3 * PL] * ir;
-            E = u[4 * PL] * ir;
-          } else {
-            v0 = u[PL] / rho; v1 = u[2 * PL] / rho; v2 = u[3 * PL] / rho;
-            E = u[4 * PL] / rho;
-          }
-          pw[it] = ((gam - Real(1)) * rho) * (E - (((v0 * v0) + (v1 * v1)) + (v2 * v2)) / Real(2));
+      // P on plane K+2, tile + 2 (navier_stokes.py:94-100); with viscosity it
+      // is formed inside the stress loop below (same cells)
+      Real* const pw = pring + pmod(flat ? K : K + 2, 3) * PL2;
+      const Real* const usrc = flat ? uK : uK2;
+      auto pressure_at = [&](int it) {
+        const int r2 = it / W2, c2 = it % W2;
+        const Real* u = usrc + (r2 + HH - 2) * W + c2 + 2;
+        const Real rho = u[0];
+        Real v0, v1, v2, E;
+        if constexpr (F32) {
+          const Real ir = rcp_approx(rho);
+          v0 = u[PL] * ir; v1 = u[2 * PL] * ir; v2 = u[3 * PL] * ir;
+          E = u[4 * PL] * ir;
+        } else {
+          v0 = u[PL] / rho; v1 = u[2 * PL] / rho; v2 = u[3 * PL] / rho;
+          E = u[4 * PL] / rho;
         }
+        pw[it] = ((gam - Real(1)) * rho) * (E - (((v0 * v0) + (v1 * v1)) + (v2 * v2)) / Real(2));
+      };
+      if constexpr (!VISC) {
+        for (int it = tid; it < C::PL2; it += NT) pressure_at(it);
+      } else {
+        __syncthreads();  // v of plane K+3 (phase B) before the stress loop
       }
-      if constexpr (VISC) __syncthreads();
       // ---------------------------------------------------------- D ----
       // Stokes stress on plane K+2, tile + 2, zero on ghosts (:102-142)
       if constexpr (VISC) {
@@ -345,6 +348,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         const Real* vp = vring + pmod(pl + 1, 3) * 3 * PL;
         Real* tw = tring + pmod(pl, 3) * 6 * PL2;
         for (int it = tid; it < C::PL2; it += NT) {
+          pressure_at(it);
           const int r2 = it / W2, c2 = it % W2;
           const int r = r2 + 1, c = c2 + 2;
           const int i = x0 + c2 - 2, j = y0 + r2 - 2;
