@@ -162,16 +162,20 @@ struct ConvCfg {
   static constexpr int WB = 27 * CIN * COUT * 2;
   static constexpr int OFF_W = 0;
   static constexpr int OFF_RING = WB;
-  static constexpr int OFF_BAR = OFF_RING + NSLOT * PLANEB;
+  static constexpr int OFF_BIAS = OFF_RING + NSLOT * PLANEB;
+  static constexpr int OFF_BAR = OFF_BIAS + COUT * 4;
   static constexpr int BYTES = OFF_BAR + 64;
   static constexpr int ELEMS = YE * XE * NCH;
   static constexpr int PER = (ELEMS + 127) / 128;
   static constexpr int TCOLS = 2 * COUT < 32 ? 32 : 2 * COUT;
+  // CTAs per SM that shared memory allows (227 KB usable, 1 KB reserved each),
+  // at most four: the register budget the compiler may use follows from it
+  static constexpr int MINB = (227 * 1024) / (BYTES + 1024) > 4 ? 4 : (227 * 1024) / (BYTES + 1024);
   static_assert(WB % 128 == 0 && PLANEB % 16 == 0, "alignment");
 };
 
 template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(128, 1) conv3_kernel(const ConvArgs a) {
+__global__ void __launch_bounds__(128, ConvCfg<CIN, COUT>::MINB) conv3_kernel(const ConvArgs a) {
   using C = ConvCfg<CIN, COUT>;
   extern __shared__ __align__(128) uint8_t smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + C::OFF_BAR);  // [0] weights, [1],[2] accumulators
@@ -193,6 +197,9 @@ __global__ void __launch_bounds__(128, 1) conv3_kernel(const ConvArgs a) {
     tmem_alloc(tslot, C::TCOLS);
     tmem_relinquish();
   }
+  if constexpr (EPI != EPI_MASK_BF16) {
+    if (tid < COUT) reinterpret_cast<float*>(smem + C::OFF_BIAS)[tid] = __ldg(a.bias + tid);
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -202,31 +209,34 @@ __global__ void __launch_bounds__(128, 1) conv3_kernel(const ConvArgs a) {
     bulk_g2s(smem + C::OFF_W, a.wpack, C::WB, &bar[0]);
   }
 
+  // The (periodic) x-y offsets of this thread's plane elements do not depend
+  // on z: decompose them once.
   uint4 reg[C::PER];
-  auto load_plane = [&](int z) {
-    z = (z + n3) % n3;
+  int goff[C::PER], soff[C::PER];
 #pragma unroll
-    for (int u = 0; u < C::PER; ++u) {
-      const int e = tid + u * 128;
-      if (e < C::ELEMS) {
-        const int r = e / (C::XE * C::NCH), rem = e - r * (C::XE * C::NCH);
-        const int xe = rem / C::NCH, c = rem - xe * C::NCH;
-        const int y = (y0 - 1 + r + n2) % n2, x = (x0 - 1 + xe + n1) % n1;
-        reg[u] = ldg16(a.x + ((((size_t)z * n2 + y) * n1 + x) * CIN + c * 8));
-      }
-    }
+  for (int u = 0; u < C::PER; ++u) {
+    const int e = tid + u * 128;
+    const int r = e / (C::XE * C::NCH), rem = e - r * (C::XE * C::NCH);
+    const int xe = rem / C::NCH, c = rem - xe * C::NCH;
+    int y = y0 - 1 + r, x = x0 - 1 + xe;
+    y = y < 0 ? y + n2 : (y >= n2 ? y - n2 : y);
+    x = x < 0 ? x + n1 : (x >= n1 ? x - n1 : x);
+    goff[u] = (y * n1 + x) * CIN + c * 8;
+    soff[u] = ((r * C::NCH + c) * C::XE + xe) * 16;
+  }
+  const size_t zstride = (size_t)n2 * n1 * CIN;
+  auto load_plane = [&](int z) {
+    z = z < 0 ? z + n3 : (z >= n3 ? z - n3 : z);
+    const __nv_bfloat16* zb = a.x + (size_t)z * zstride;
+#pragma unroll
+    for (int u = 0; u < C::PER; ++u)
+      if (tid + u * 128 < C::ELEMS) reg[u] = ldg16(zb + goff[u]);
   };
   auto store_plane = [&](int slot) {
     uint8_t* base = smem + C::OFF_RING + slot * C::PLANEB;
 #pragma unroll
-    for (int u = 0; u < C::PER; ++u) {
-      const int e = tid + u * 128;
-      if (e < C::ELEMS) {
-        const int r = e / (C::XE * C::NCH), rem = e - r * (C::XE * C::NCH);
-        const int xe = rem / C::NCH, c = rem - xe * C::NCH;
-        sts16(base + ((r * C::NCH + c) * C::XE + xe) * 16, reg[u]);
-      }
-    }
+    for (int u = 0; u < C::PER; ++u)
+      if (tid + u * 128 < C::ELEMS) sts16(base + soff[u], reg[u]);
   };
   for (int j = 0; j < 3; ++j) {
     load_plane(z0 - 1 + j);
@@ -243,6 +253,7 @@ __global__ void __launch_bounds__(128, 1) conv3_kernel(const ConvArgs a) {
   constexpr uint32_t IDESC = idesc_bf16(128, COUT, 0, 0);
   int pending[2] = {-1, -1};  // committed, not yet waited step per accumulator buffer
   const int m = warp * 32 + lane, xl = m & 7, yl = m >> 3;
+  const float* bias = reinterpret_cast<const float*>(smem + C::OFF_BIAS);
 
   auto epilogue = [&](int s) {
     const int b = s & 1;
@@ -261,10 +272,9 @@ __global__ void __launch_bounds__(128, 1) conv3_kernel(const ConvArgs a) {
       float4* out = reinterpret_cast<float4*>(static_cast<float*>(a.y) + pos * COUT);
 #pragma unroll
       for (int q = 0; q < COUT / 4; ++q)
-        out[q] = make_float4(__uint_as_float(v[4 * q]) + __ldg(a.bias + 4 * q),
-                             __uint_as_float(v[4 * q + 1]) + __ldg(a.bias + 4 * q + 1),
-                             __uint_as_float(v[4 * q + 2]) + __ldg(a.bias + 4 * q + 2),
-                             __uint_as_float(v[4 * q + 3]) + __ldg(a.bias + 4 * q + 3));
+        out[q] = make_float4(__uint_as_float(v[4 * q]) + bias[4 * q], __uint_as_float(v[4 * q + 1]) + bias[4 * q + 1],
+                             __uint_as_float(v[4 * q + 2]) + bias[4 * q + 2],
+                             __uint_as_float(v[4 * q + 3]) + bias[4 * q + 3]);
     } else {
       uint4* out = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.y) + pos * COUT);
 #pragma unroll
@@ -274,7 +284,7 @@ __global__ void __launch_bounds__(128, 1) conv3_kernel(const ConvArgs a) {
         for (int e = 0; e < 8; ++e) f[e] = __uint_as_float(v[8 * q + e]);
         if constexpr (EPI == EPI_RELU_BF16) {
 #pragma unroll
-          for (int e = 0; e < 8; ++e) f[e] = fmaxf(f[e] + __ldg(a.bias + 8 * q + e), 0.f);
+          for (int e = 0; e < 8; ++e) f[e] = fmaxf(f[e] + bias[8 * q + e], 0.f);
         } else {
           const uint4 mk = ldg16(a.mask + pos * COUT + 8 * q);
           const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
@@ -401,54 +411,52 @@ __global__ void __launch_bounds__(128, 1) wgrad_kernel(const WgradArgs a) {
   tc_fence_after();
   const uint32_t tbase = *tslot;
 
+  // z-independent element offsets, decomposed once (periodic wrap in x, y)
   uint4 xr[C::XPER], gr[C::GPER];
-  auto load_x = [&](int z) {
-    z = (z + n3) % n3;
+  int xg[C::XPER], xs[C::XPER], gg[C::GPER], gs[C::GPER];
 #pragma unroll
-    for (int u = 0; u < C::XPER; ++u) {
-      const int e = tid + u * 128;
-      if (e < C::XELEMS) {
-        const int r = e / (C::XE * C::NCH), rem = e - r * (C::XE * C::NCH);
-        const int xe = rem / C::NCH, c = rem - xe * C::NCH;
-        const int y = (y0 - 1 + r + n2) % n2, x = (x0 - 1 + xe + n1) % n1;
-        xr[u] = ldg16(a.x + ((((size_t)z * n2 + y) * n1 + x) * CIN + c * 8));
-      }
-    }
+  for (int u = 0; u < C::XPER; ++u) {
+    const int e = tid + u * 128;
+    const int r = e / (C::XE * C::NCH), rem = e - r * (C::XE * C::NCH);
+    const int xe = rem / C::NCH, c = rem - xe * C::NCH;
+    int y = y0 - 1 + r, x = x0 - 1 + xe;
+    y = y < 0 ? y + n2 : (y >= n2 ? y - n2 : y);
+    x = x < 0 ? x + n1 : (x >= n1 ? x - n1 : x);
+    xg[u] = (y * n1 + x) * CIN + c * 8;
+    xs[u] = ((r * C::NCH + c) * C::XE + xe) * 16;
+  }
+#pragma unroll
+  for (int u = 0; u < C::GPER; ++u) {
+    const int e = tid + u * 128;
+    const int r = e / (C::TX * C::NCHG), rem = e - r * (C::TX * C::NCHG);
+    const int xe = rem / C::NCHG, c = rem - xe * C::NCHG;
+    gg[u] = ((y0 + r) * n1 + (x0 + xe)) * COUT + c * 8;
+    gs[u] = ((r * C::NCHG + c) * C::TX + xe) * 16;
+  }
+  auto load_x = [&](int z) {
+    z = z < 0 ? z + n3 : (z >= n3 ? z - n3 : z);
+    const __nv_bfloat16* zb = a.x + (size_t)z * n2 * n1 * CIN;
+#pragma unroll
+    for (int u = 0; u < C::XPER; ++u)
+      if (tid + u * 128 < C::XELEMS) xr[u] = ldg16(zb + xg[u]);
   };
   auto store_x = [&](int slot) {
     uint8_t* base = smem + C::OFF_X + slot * C::PLANEB;
 #pragma unroll
-    for (int u = 0; u < C::XPER; ++u) {
-      const int e = tid + u * 128;
-      if (e < C::XELEMS) {
-        const int r = e / (C::XE * C::NCH), rem = e - r * (C::XE * C::NCH);
-        const int xe = rem / C::NCH, c = rem - xe * C::NCH;
-        sts16(base + ((r * C::NCH + c) * C::XE + xe) * 16, xr[u]);
-      }
-    }
+    for (int u = 0; u < C::XPER; ++u)
+      if (tid + u * 128 < C::XELEMS) sts16(base + xs[u], xr[u]);
   };
   auto load_g = [&](int z) {
+    const __nv_bfloat16* zb = a.g + (size_t)z * n2 * n1 * COUT;
 #pragma unroll
-    for (int u = 0; u < C::GPER; ++u) {
-      const int e = tid + u * 128;
-      if (e < C::GELEMS) {
-        const int r = e / (C::TX * C::NCHG), rem = e - r * (C::TX * C::NCHG);
-        const int xe = rem / C::NCHG, c = rem - xe * C::NCHG;
-        gr[u] = ldg16(a.g + ((((size_t)z * n2 + (y0 + r)) * n1 + (x0 + xe)) * COUT + c * 8));
-      }
-    }
+    for (int u = 0; u < C::GPER; ++u)
+      if (tid + u * 128 < C::GELEMS) gr[u] = ldg16(zb + gg[u]);
   };
   auto store_g = [&](int slot) {
     uint8_t* base = smem + C::OFF_G + slot * C::GPLANEB;
 #pragma unroll
-    for (int u = 0; u < C::GPER; ++u) {
-      const int e = tid + u * 128;
-      if (e < C::GELEMS) {
-        const int r = e / (C::TX * C::NCHG), rem = e - r * (C::TX * C::NCHG);
-        const int xe = rem / C::NCHG, c = rem - xe * C::NCHG;
-        sts16(base + ((r * C::NCHG + c) * C::TX + xe) * 16, gr[u]);
-      }
-    }
+    for (int u = 0; u < C::GPER; ++u)
+      if (tid + u * 128 < C::GELEMS) sts16(base + gs[u], gr[u]);
   };
   for (int j = 0; j < 3; ++j) {
     load_x(z0 - 1 + j);
