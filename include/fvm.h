@@ -66,7 +66,8 @@ extern "C" {
  * params: navier_stokes {gamma, mu, g1, g2, g3}; heat {rho, cp, k, q};
  *         maxwell {mu, epsilon, sigma, rho_c, chi_B, chi_D}.
  * bc_kind/bc_value: [variable][side], sides ordered left,right,bottom,top,front,back
- * (src/solver.py:36).  tile_ty / zchunk: 0 = autotuned default. */
+ * (src/solver.py:36).  tile_ty: tile rows, 0 = the default shape (or the alternative
+ * one that fvm_tiling reports after fvm_autotune); zchunk: planes per tile, 0 = 64. */
 typedef struct fvm_desc {
   int physics, precision, coords;
   int nx1, nx2, nx3;
@@ -146,9 +147,14 @@ int fvm_clear_status(fvm_handle* h);
 int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_kernel_ms,
                       double* other_kernel_ms, int* stage_launches);
 
-/* Pick the z-march depth (planes per tile) by timing the candidates on this grid;
- * the state and clock are restored afterwards.  New: the reference has no tuning. */
+/* Pick the block shape -- tile rows (the default and, for float32
+ * navier_stokes and heat, a 4-row tile) and the z-march depth (planes per
+ * tile) -- by timing every pair on this grid; the state and clock are restored
+ * afterwards.  New: the reference has no tuning. */
 int fvm_autotune(fvm_handle* h, int* best_zchunk, double* best_ms_per_step);
+/* The handle's block shape: tile rows (fvm_desc.tile_ty, or the autotuner's
+ * choice) and z-march depth.  New: the reference has no tuning. */
+int fvm_tiling(fvm_handle* h, int* tile_ty, int* zchunk);
 
 /* Sharp Kelvin-Helmholtz initial state written on the device (the host
  * initializer of setups/kelvin_helmholtz_sharp.py, done in HBM instead of on

@@ -67,6 +67,7 @@ SIGNATURES = [
     ("fvm_last_error", C.c_int, [C.c_char_p, C.c_int]),
     ("fvm_totals_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p]),
     ("fvm_autotune", C.c_int, [_P, C.POINTER(C.c_int), _DP]),
+    ("fvm_tiling", C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("fvm_batch_create", C.c_int, [C.POINTER(FvmDesc), C.c_int, C.POINTER(_P)]),
     ("fvm_batch_destroy", C.c_int, [_P]),
     ("fvm_batch_size", C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),

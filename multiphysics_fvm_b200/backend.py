@@ -270,6 +270,12 @@ class Simulation:
         L.check(self._lib.fvm_autotune(self._h, C.byref(z), C.byref(ms)), "fvm_autotune")
         return z.value, ms.value
 
+    def tiling(self):
+        """(tile rows, z-march depth) the stage kernels run with."""
+        ty, z = C.c_int(), C.c_int()
+        L.check(self._lib.fvm_tiling(self._h, C.byref(ty), C.byref(z)), "fvm_tiling")
+        return ty.value, z.value
+
     def info(self):
         nv, nb = C.c_int(), C.c_longlong()
         L.check(self._lib.fvm_info(self._h, C.byref(nv), C.byref(nb)), "fvm_info")

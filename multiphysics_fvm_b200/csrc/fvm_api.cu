@@ -115,6 +115,7 @@ struct fvm_handle {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   double max_inv_l2 = 0.0, const_rate = 0.0;
   int zchunk = 64;
+  int tile_ty = 0;  // tile rows of the stage kernel (its tensor maps are built for it)
   long long device_bytes = 0;
   fvm_closure* closure = nullptr;  // learned flux correction run inside every step
   double closure_beta = 0.5;
@@ -122,6 +123,10 @@ struct fvm_handle {
 };
 
 namespace {
+
+int default_tile_ty(const fvm_desc& d);
+int alt_tile_ty(const fvm_desc& d);
+int tile_halo(const fvm_desc& d);
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -155,6 +160,14 @@ int make_tmap(fvm_handle* h, int b, int rows) {
   return FVM_OK;
 }
 
+// Tensor maps of the three state buffers for the handle's tile rows.
+int make_tmaps(fvm_handle* h) {
+  const int rows = h->tile_ty + 2 * tile_halo(h->d);
+  for (int b = 0; b < 3; ++b)
+    if (int rc = make_tmap(h, b, rows)) return rc;
+  return FVM_OK;
+}
+
 int validate(const fvm_desc* d) {
   if (!d) return fail(FVM_E_INVALID, "null desc");
   if (d->physics < FVM_NAVIER_STOKES || d->physics > FVM_MAXWELL)
@@ -168,6 +181,9 @@ int validate(const fvm_desc* d) {
   if (d->limiter < 0 || d->limiter > 2) return fail(FVM_E_INVALID, "unknown slope limiter");
   if (d->riemann < 0 || d->riemann > 1) return fail(FVM_E_INVALID, "unknown riemann solver");
   if (d->integrator < 0 || d->integrator > 3) return fail(FVM_E_INVALID, "unknown time integrator");
+  if (d->tile_ty != 0 && d->tile_ty != default_tile_ty(*d) && d->tile_ty != alt_tile_ty(*d))
+    return fail(FVM_E_INVALID, "tile_ty must be 0 (default), " + std::to_string(default_tile_ty(*d)) + " or " +
+                                   std::to_string(alt_tile_ty(*d)) + " for this physics and precision");
   const int nv = d->physics == FVM_NAVIER_STOKES ? 5 : (d->physics == FVM_HEAT ? 1 : 6);
   for (int q = 0; q < nv; ++q)
     for (int s = 0; s < 6; ++s) {
@@ -181,6 +197,27 @@ int validate(const fvm_desc* d) {
 int kernel_limiter(const fvm_desc& d) {
   if (d.reconstructor == FVM_PIECEWISE_CONSTANT) return LIM_PC;
   return d.limiter == FVM_MINMOD ? LIM_MINMOD : (d.limiter == FVM_MONOTONIZED_CENTRAL ? LIM_MC : LIM_VANLEER);
+}
+
+// Tile rows: the default block shape of the physics/precision, and the second
+// one the float32 NS and heat kernels are also built with (equal if none).
+int default_tile_ty(const fvm_desc& d) {
+  const bool f64 = d.precision == FVM_FP64, visc = d.physics == FVM_NAVIER_STOKES && d.params[1] != 0.0;
+  if (d.physics == FVM_HEAT) return HEAT_TY;
+  if (d.physics == FVM_MAXWELL) return f64 ? maxwell_tile_ty<double>() : maxwell_tile_ty<float>();
+  if (f64) return visc ? ns_tile_ty<double, true>() : ns_tile_ty<double, false>();
+  return visc ? ns_tile_ty<float, true>() : ns_tile_ty<float, false>();
+}
+int alt_tile_ty(const fvm_desc& d) {
+  if (d.precision == FVM_FP64 || d.physics == FVM_MAXWELL) return default_tile_ty(d);
+  if (d.physics == FVM_HEAT) return HEAT_TY_ALT;
+  return d.params[1] != 0.0 ? ns_tile_ty_alt<float, true>() : ns_tile_ty_alt<float, false>();
+}
+// Halo rows staged on each side of a tile (TMA box height = rows + 2*halo).
+int tile_halo(const fvm_desc& d) {
+  if (d.physics == FVM_HEAT) return d.reconstructor == FVM_PIECEWISE_CONSTANT ? 2 : 3;
+  if (d.physics == FVM_MAXWELL) return 2;
+  return d.params[1] != 0.0 ? 3 : 2;
 }
 
 BcSpec make_bc(const fvm_desc& d, int nv) {
@@ -302,7 +339,7 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
   const int nsm = prepare_only ? -1 : h->nsm;
   if (d.physics == FVM_HEAT)
     return launch_heat<Real>(kernel_limiter(d), d.coords, h->tmap[sd.in], make_heat_params<Real>(h, sd, rhs_only),
-                             h->stream, nsm);
+                             h->stream, nsm, h->tile_ty);
   if (d.physics == FVM_MAXWELL) {
     MaxwellParams<Real> p{};
     fill_common<Real>(h, sd, rhs_only, p);
@@ -317,7 +354,7 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
   }
   const bool visc = d.params[1] != 0.0;
   return launch_ns<Real>(kernel_limiter(d), d.riemann, d.coords, visc, h->tmap[sd.in],
-                         make_ns_params<Real>(h, sd, rhs_only), h->stream, nsm);
+                         make_ns_params<Real>(h, sd, rhs_only), h->stream, nsm, h->tile_ty);
 }
 
 cudaError_t launch_bc(fvm_handle* h, int b, bool use_active) {
@@ -536,15 +573,11 @@ int fvm_create(const fvm_desc* desc, fvm_handle** out) {
   FVM_CKC(cudaMallocHost(&h->stage_host, h->stage_elems * sizeof(double)));
   h->device_bytes += h->stage_elems * sizeof(double);
 #undef FVM_CKC
-  const bool visc = d.physics == FVM_NAVIER_STOKES && d.params[1] != 0.0;
-  int rows;
-  if (d.physics == FVM_HEAT) rows = 8 + (d.reconstructor == FVM_PIECEWISE_CONSTANT ? 4 : 6);
-  else if (d.physics == FVM_MAXWELL) rows = (h->f64 ? maxwell_tile_ty<double>() : maxwell_tile_ty<float>()) + 4;
-  else if (h->f64) rows = visc ? ns_tile_ty<double, true>() + 6 : ns_tile_ty<double, false>() + 4;
-  else rows = visc ? ns_tile_ty<float, true>() + 6 : ns_tile_ty<float, false>() + 4;
-  for (int b = 0; b < 3; ++b) {
-    rc = make_tmap(h, b, rows);
-    if (rc) { fvm_destroy(h); return rc; }
+  h->tile_ty = d.tile_ty > 0 ? d.tile_ty : default_tile_ty(d);
+  rc = make_tmaps(h);
+  if (rc) {
+    fvm_destroy(h);
+    return rc;
   }
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
     fvm_destroy(h);
@@ -1109,7 +1142,9 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     return bail(fail(FVM_E_CUDA, "stream creation failed"));
   for (int i = 0; i < n; ++i) {
     fvm_handle* h = nullptr;
-    const int rc = fvm_create(&descs[i], &h);
+    fvm_desc di = descs[i];
+    di.tile_ty = 0;  // the batched kernels use each physics' default block shape
+    const int rc = fvm_create(&di, &h);
     if (rc) return bail(rc);
     b->h.push_back(h);
   }
@@ -1277,26 +1312,43 @@ int fvm_autotune(fvm_handle* h, int* best_zchunk, double* best_ms) {
   Saved sv;
   int rc = save_states({h}, sv);
   if (rc) return rc;
-  int best = h->zchunk;
+  int best = h->zchunk, best_ty = h->tile_ty;
   double bt = 1e30;
-  for (int z : zchunk_candidates(h->d.nx3)) {
-    h->zchunk = z;
-    for (auto& g : h->graph)
-      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
-    double ms = 0.0;
-    if ((rc = fvm_time_steps(h, 1, 0, &ms))) break;  // warm-up (builds the graph)
-    if ((rc = fvm_time_steps(h, 3, 0, &ms))) break;
-    if (ms < bt) { bt = ms; best = z; }
-    if ((rc = restore_states({h}, sv, false))) break;
+  std::vector<int> tys{default_tile_ty(h->d)};
+  if (alt_tile_ty(h->d) != tys[0]) tys.push_back(alt_tile_ty(h->d));
+  for (int ty : tys) {
+    h->tile_ty = ty;
+    if ((rc = make_tmaps(h))) break;
+    for (int z : zchunk_candidates(h->d.nx3)) {
+      h->zchunk = z;
+      for (auto& g : h->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+      double ms = 0.0;
+      if ((rc = fvm_time_steps(h, 1, 0, &ms))) break;  // warm-up (builds the graph)
+      if ((rc = fvm_time_steps(h, 3, 0, &ms))) break;
+      if (ms < bt) { bt = ms; best = z; best_ty = ty; }
+      if ((rc = restore_states({h}, sv, false))) break;
+    }
+    if (rc) break;
   }
   const int rr = restore_states({h}, sv, true);
   h->zchunk = best;
+  h->tile_ty = best_ty;
+  const int rt = make_tmaps(h);
   for (auto& g : h->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   if (rc) return rc;
   if (rr) return rr;
+  if (rt) return rt;
   if (best_zchunk) *best_zchunk = best;
   if (best_ms) *best_ms = bt / 3.0;
+  return FVM_OK;
+}
+
+int fvm_tiling(fvm_handle* h, int* tile_ty, int* zchunk) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  if (tile_ty) *tile_ty = h->tile_ty;
+  if (zchunk) *zchunk = h->zchunk;
   return FVM_OK;
 }
 

@@ -13,8 +13,16 @@ namespace fvm {
 // float32 inviscid 8 rows (2 blocks), float64 viscous 4 rows, inviscid 8.
 template <typename Real, bool VISC>
 constexpr int ns_tile_ty() { return std::is_same<Real, double>::value ? (VISC ? 4 : 8) : (VISC ? 6 : 8); }
+// The float32 kernels also come with 4-row tiles (a second block shape for
+// the autotuner: fewer threads and less shared memory per block, more halo
+// per cell); float64 has the default shape only.
 template <typename Real, bool VISC>
-constexpr int ns_min_blocks() { return std::is_same<Real, double>::value ? 1 : (VISC ? 2 : 3); }
+constexpr int ns_tile_ty_alt() { return std::is_same<Real, double>::value ? ns_tile_ty<Real, VISC>() : 4; }
+template <typename Real, bool VISC, int TY = ns_tile_ty<Real, VISC>()>
+constexpr int ns_min_blocks() {
+  return std::is_same<Real, double>::value ? 1 : (VISC ? 2 : (TY == 8 ? 3 : 4));
+}
+constexpr int HEAT_TY = 8, HEAT_TY_ALT = 4;
 
 template <typename K>
 static cudaError_t prepare_kernel(K kern, int threads, int bytes, int* blocks_per_sm) {
@@ -32,11 +40,10 @@ static cudaError_t prepare_kernel(K kern, int threads, int bytes, int* blocks_pe
 
 // nsm < 0: only set the kernel's shared-memory attribute and query its
 // occupancy (done once, outside any stream capture).
-template <typename Real, int LIM, int RIEM, int COORD, bool VISC, class Src>
+template <typename Real, int LIM, int RIEM, int COORD, bool VISC, class Src, int TY = ns_tile_ty<Real, VISC>()>
 cudaError_t launch_ns_src(const Src& src, long long ntiles, cudaStream_t s, int nsm) {
-  constexpr int TY = ns_tile_ty<Real, VISC>();
   using C = NsCfg<Real, VISC, TY>;
-  auto kern = ns_stage_kernel<Real, LIM, RIEM, COORD, VISC, TY, ns_min_blocks<Real, VISC>(), Src>;
+  auto kern = ns_stage_kernel<Real, LIM, RIEM, COORD, VISC, TY, ns_min_blocks<Real, VISC, TY>(), Src>;
   static int bps = 0;
   if (bps == 0 || nsm < 0) {
     cudaError_t e = prepare_kernel(kern, C::NT, C::BYTES, &bps);
@@ -50,29 +57,38 @@ cudaError_t launch_ns_src(const Src& src, long long ntiles, cudaStream_t s, int 
 }
 
 template <typename Real, bool VISC>
-void ns_tile_counts(NsParams<Real>& p) {
-  constexpr int TY = ns_tile_ty<Real, VISC>();
+void ns_tile_counts(NsParams<Real>& p, int ty = ns_tile_ty<Real, VISC>()) {
   p.ntx = (p.lay.nx + 31) / 32;
-  p.nty = (p.lay.ny + TY - 1) / TY;
+  p.nty = (p.lay.ny + ty - 1) / ty;
   p.nzc = p.flat ? 1 : (p.lay.nz + p.zchunk - 1) / p.zchunk;
 }
 
+// ty: tile rows of the handle (its tensor maps were built for it).
 template <typename Real, int LIM, int RIEM, int COORD, bool VISC>
-cudaError_t launch_ns_one(const CUtensorMap& map, NsParams<Real> p, cudaStream_t s, int nsm) {
-  ns_tile_counts<Real, VISC>(p);
+cudaError_t launch_ns_one(const CUtensorMap& map, NsParams<Real> p, cudaStream_t s, int nsm, int ty) {
+  constexpr int TD = ns_tile_ty<Real, VISC>(), TA = ns_tile_ty_alt<Real, VISC>();
   SingleSource<NsParams<Real>> src;
   src.tmap = map;
+  if constexpr (TA != TD) {
+    if (ty == TA) {
+      ns_tile_counts<Real, VISC>(p, TA);
+      src.p = p;
+      return launch_ns_src<Real, LIM, RIEM, COORD, VISC, SingleSource<NsParams<Real>>, TA>(
+          src, (long long)p.ntx * p.nty * p.nzc, s, nsm);
+    }
+  }
+  ns_tile_counts<Real, VISC>(p, TD);
   src.p = p;
   return launch_ns_src<Real, LIM, RIEM, COORD, VISC>(src, (long long)p.ntx * p.nty * p.nzc, s, nsm);
 }
 
 template <typename Real, int COORD>
 cudaError_t launch_ns_coord(int lim, int riem, bool visc, const CUtensorMap& map, const NsParams<Real>& p,
-                            cudaStream_t s, int nsm) {
+                            cudaStream_t s, int nsm, int ty) {
 #define FVM_NS_CASE(L, R)                                                          \
   if (lim == L && riem == R)                                                       \
-    return visc ? launch_ns_one<Real, L, R, COORD, true>(map, p, s, nsm)           \
-                : launch_ns_one<Real, L, R, COORD, false>(map, p, s, nsm);
+    return visc ? launch_ns_one<Real, L, R, COORD, true>(map, p, s, nsm, ty)       \
+                : launch_ns_one<Real, L, R, COORD, false>(map, p, s, nsm, ty);
   FVM_NS_CASE(LIM_PC, RIEM_RUSANOV)
   FVM_NS_CASE(LIM_PC, RIEM_HLL)
   FVM_NS_CASE(LIM_MINMOD, RIEM_RUSANOV)
@@ -109,7 +125,7 @@ cudaError_t launch_ns_batch_coord(int lim, int riem, bool visc, const BatchSourc
 // Declarations of the per-(precision, coordinate) instantiations.
 #define FVM_DECLARE_NS(REAL, COORD)                                                                      \
   extern template cudaError_t launch_ns_coord<REAL, COORD>(int, int, bool, const CUtensorMap&,          \
-                                                          const NsParams<REAL>&, cudaStream_t, int);    \
+                                                          const NsParams<REAL>&, cudaStream_t, int, int); \
   extern template cudaError_t launch_ns_batch_coord<REAL, COORD>(                                        \
       int, int, bool, const BatchSource<NsParams<REAL>>&, long long, cudaStream_t, int);
 FVM_DECLARE_NS(float, COORD_CART)
@@ -129,16 +145,15 @@ cudaError_t launch_ns_batch(int lim, int riem, int coord, bool visc, const Batch
 
 template <typename Real>
 cudaError_t launch_ns(int lim, int riem, int coord, bool visc, const CUtensorMap& map, const NsParams<Real>& p,
-                      cudaStream_t s, int nsm) {
-  if (coord == COORD_CART) return launch_ns_coord<Real, COORD_CART>(lim, riem, visc, map, p, s, nsm);
-  if (coord == COORD_CYL) return launch_ns_coord<Real, COORD_CYL>(lim, riem, visc, map, p, s, nsm);
-  return launch_ns_coord<Real, COORD_SPH>(lim, riem, visc, map, p, s, nsm);
+                      cudaStream_t s, int nsm, int ty) {
+  if (coord == COORD_CART) return launch_ns_coord<Real, COORD_CART>(lim, riem, visc, map, p, s, nsm, ty);
+  if (coord == COORD_CYL) return launch_ns_coord<Real, COORD_CYL>(lim, riem, visc, map, p, s, nsm, ty);
+  return launch_ns_coord<Real, COORD_SPH>(lim, riem, visc, map, p, s, nsm, ty);
 }
 
 // ---------------------------------------------------------------- heat ----
-template <typename Real, int LIM, int COORD, class Src>
+template <typename Real, int LIM, int COORD, class Src, int TY = HEAT_TY>
 cudaError_t launch_heat_src(const Src& src, long long ntiles, cudaStream_t s, int nsm) {
-  constexpr int TY = 8;
   using C = HeatCfg<Real, LIM, TY>;
   auto kern = heat_stage_kernel<Real, LIM, COORD, TY, Src>;
   static int bps = 0;
@@ -153,19 +168,19 @@ cudaError_t launch_heat_src(const Src& src, long long ntiles, cudaStream_t s, in
 }
 
 template <typename Real>
-void heat_tile_counts(HeatParams<Real>& p) {
+void heat_tile_counts(HeatParams<Real>& p, int ty = HEAT_TY) {
   p.ntx = (p.lay.nx + 31) / 32;
-  p.nty = (p.lay.ny + 7) / 8;
+  p.nty = (p.lay.ny + ty - 1) / ty;
   p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
 }
 
-template <typename Real, class Src>
+template <typename Real, class Src, int TY = HEAT_TY>
 cudaError_t launch_heat_any(int lim, int coord, const Src& src, long long ntiles, cudaStream_t s, int nsm) {
 #define FVM_HEAT_CASE(L)                                                                               \
   if (lim == L) {                                                                                      \
-    if (coord == COORD_CART) return launch_heat_src<Real, L, COORD_CART>(src, ntiles, s, nsm);         \
-    if (coord == COORD_CYL) return launch_heat_src<Real, L, COORD_CYL>(src, ntiles, s, nsm);           \
-    return launch_heat_src<Real, L, COORD_SPH>(src, ntiles, s, nsm);                                   \
+    if (coord == COORD_CART) return launch_heat_src<Real, L, COORD_CART, Src, TY>(src, ntiles, s, nsm); \
+    if (coord == COORD_CYL) return launch_heat_src<Real, L, COORD_CYL, Src, TY>(src, ntiles, s, nsm);   \
+    return launch_heat_src<Real, L, COORD_SPH, Src, TY>(src, ntiles, s, nsm);                           \
   }
   FVM_HEAT_CASE(LIM_PC)
   FVM_HEAT_CASE(LIM_MINMOD)
@@ -177,11 +192,19 @@ cudaError_t launch_heat_any(int lim, int coord, const Src& src, long long ntiles
 
 template <typename Real>
 cudaError_t launch_heat(int lim, int coord, const CUtensorMap& map, const HeatParams<Real>& p0, cudaStream_t s,
-                        int nsm) {
+                        int nsm, int ty) {
   HeatParams<Real> p = p0;
-  heat_tile_counts(p);
   SingleSource<HeatParams<Real>> src;
   src.tmap = map;
+  if constexpr (std::is_same<Real, float>::value) {
+    if (ty == HEAT_TY_ALT) {
+      heat_tile_counts(p, HEAT_TY_ALT);
+      src.p = p;
+      return launch_heat_any<Real, SingleSource<HeatParams<Real>>, HEAT_TY_ALT>(
+          lim, coord, src, (long long)p.ntx * p.nty * p.nzc, s, nsm);
+    }
+  }
+  heat_tile_counts(p);
   src.p = p;
   return launch_heat_any<Real>(lim, coord, src, (long long)p.ntx * p.nty * p.nzc, s, nsm);
 }
@@ -190,8 +213,10 @@ cudaError_t launch_heat_batch(int lim, int coord, const BatchSource<HeatParams<R
                               cudaStream_t s, int nsm) {
   return launch_heat_any<Real>(lim, coord, src, ntiles, s, nsm);
 }
-extern template cudaError_t launch_heat<float>(int, int, const CUtensorMap&, const HeatParams<float>&, cudaStream_t, int);
-extern template cudaError_t launch_heat<double>(int, int, const CUtensorMap&, const HeatParams<double>&, cudaStream_t, int);
+extern template cudaError_t launch_heat<float>(int, int, const CUtensorMap&, const HeatParams<float>&, cudaStream_t, int,
+                                              int);
+extern template cudaError_t launch_heat<double>(int, int, const CUtensorMap&, const HeatParams<double>&, cudaStream_t,
+                                               int, int);
 extern template cudaError_t launch_heat_batch<float>(int, int, const BatchSource<HeatParams<float>>&, long long,
                                                      cudaStream_t, int);
 extern template cudaError_t launch_heat_batch<double>(int, int, const BatchSource<HeatParams<double>>&, long long,

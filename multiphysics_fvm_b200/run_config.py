@@ -6,7 +6,8 @@
 Configurations: kh2d (2D sharp Kelvin-Helmholtz), kh3d (its 3D extrusion),
 rt3d (3D Rayleigh-Taylor), maxwell_sph (spherical pulse), heat_cyl
 (cylindrical hot spot), batch_c3 (96 mixed grids in one batch).  Prints the
-device time per step; --autotune picks the z-march depth first.
+device time per step; --autotune picks the block shape (tile rows, z-march
+depth) first.
 """
 from __future__ import annotations
 
@@ -82,7 +83,7 @@ def main():
     sim.step(a.warmup)
     ms = sim.time_steps(a.steps)
     if tuned:
-        print(f"autotuned z-march depth {tuned[0]} ({tuned[1]:.3f} ms/step in the sweep)")
+        print(f"autotuned tile rows {sim.tiling()[0]}, z-march depth {tuned[0]} ({tuned[1]:.3f} ms/step in the sweep)")
     print(f"{a.config} n={a.n} {s.get('precision')}: {ms / a.steps:.3f} ms/step, status={sim.status()}")
 
 
