@@ -172,22 +172,24 @@ __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, co
     const long long g0 = L.idx(0, k + 1, j + 1, 1);
    for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
     const long long g = g0 + i;
+    // float64 throughout; one reciprocal of rho and the inverse-length tables
+    // replace the eight divisions (dt moves by ulps, inside the 1e-12 bound)
     const double rho = double(u[g]);
-    const double v0 = double(u[g + L.var_stride]) / rho, v1 = double(u[g + 2 * L.var_stride]) / rho,
-                 v2 = double(u[g + 3 * L.var_stride]) / rho;
-    const double E = double(u[g + 4 * L.var_stride]) / rho;
+    const double ir = 1.0 / rho;
+    const double v0 = double(u[g + L.var_stride]) * ir, v1 = double(u[g + 2 * L.var_stride]) * ir,
+                 v2 = double(u[g + 3 * L.var_stride]) * ir;
+    const double E = double(u[g + 4 * L.var_stride]) * ir;
     const double P = ((gam - 1.0) * rho) * (E - (((v0 * v0) + (v1 * v1)) + (v2 * v2)) / 2.0);
-    const double cs = sqrt((gam * P) / rho);
+    const double cs = sqrt((gam * P) * ir);
     if (!(rho > 0.0)) bad |= ST_DENSITY;
     if (!(P > 0.0)) bad |= ST_PRESSURE;
     const double vv[3] = {v0, v1, v2};
     double ml[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) ml[d] = fmax(fmax(fabs(vv[d] + 0.0), fabs(vv[d] + (-cs))), fabs(vv[d] + cs));
-    const double l1 = Geo<double, COORD>::L1(m, i, j, k), l2 = Geo<double, COORD>::L2(m, i, j, k),
-                 l3 = Geo<double, COORD>::L3(m, i, j, k);
-    const double r = fmax(fmax(ml[0] / l1, ml[1] / l2), ml[2] / l3);
-    const double nl = mu / rho;
+    const double r = fmax(fmax(ml[0] * inv_len<double, COORD, 0>(m, i, j, k), ml[1] * inv_len<double, COORD, 1>(m, i, j, k)),
+                          ml[2] * inv_len<double, COORD, 2>(m, i, j, k));
+    const double nl = mu * ir;
     if (!(r >= 0.0) || !(nl >= 0.0)) bad |= ST_NONFINITE;
     rc = fmax(rc, r);
     nu = fmax(nu, nl);
