@@ -31,7 +31,9 @@ struct HeatParams {
 template <typename Real, int LIM, int TY>
 struct HeatCfg {
   static constexpr int TX = 32;
-  static constexpr int NT = TX * (TY + 2);
+  // enough threads for one phi task each over the tile + 1 halo, and for the
+  // (TY+2) x TX x2-face tasks
+  static constexpr int NT = round_up((TX + 2) * (TY + 2), 32);
   static constexpr int HH = LIM == LIM_PC ? 2 : 3;
   static constexpr int W = 40;
   static constexpr int ROWS = TY + 2 * HH;
@@ -126,27 +128,29 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         phase_bits ^= 1u << s;
         pending &= ~(1u << s);
       }
-      // T on the newest plane (heat.py:74)
-      {
+      // T on the newest plane (heat.py:74).  T = U / (rho cp) is linear in U,
+      // so the float32 path differences the U ring directly and folds
+      // 1/(rho cp) into the gradient factor (no T ring, no barrier); float64
+      // keeps the reference's T = U / (rho cp) first.
+      if constexpr (!F32) {
         const int pl = K + HH;
         const Real* ub = uring + pmod(pl, C::NSLOT) * C::SLOT;
         Real* tb = tring + pmod(pl, 3) * PL;
         for (int it = tid; it < C::ROWS * (TX + 6); it += NT) {
           const int o = (it / (TX + 6)) * W + 1 + it % (TX + 6);
-          if constexpr (F32) tb[o] = ub[o] * ircp;
-          else tb[o] = ub[o] / rcp;
+          tb[o] = ub[o] / rcp;
         }
+        __syncthreads();
       }
-      __syncthreads();
       // phi = -k grad T on plane K+HH-1 (heat.py:85-95), zero on ghosts, over
       // the tile plus PH = HH-1 cells (what the x1/x2 face states read)
       if (K >= Z0 - 2 * HH + 2) {
         constexpr int PH = HH - 1;
         const int pl = K + HH - 1, k = pl - 1;
         const bool zg = k < 0 || k >= nz;
-        const Real* tm = tring + pmod(pl - 1, 3) * PL;
-        const Real* t0 = tring + pmod(pl, 3) * PL;
-        const Real* tp = tring + pmod(pl + 1, 3) * PL;
+        const Real* tm = F32 ? uring + pmod(pl - 1, C::NSLOT) * C::SLOT : tring + pmod(pl - 1, 3) * PL;
+        const Real* t0 = F32 ? uring + pmod(pl, C::NSLOT) * C::SLOT : tring + pmod(pl, 3) * PL;
+        const Real* tp = F32 ? uring + pmod(pl + 1, C::NSLOT) * C::SLOT : tring + pmod(pl + 1, 3) * PL;
         Real* pw = phring + pmod(pl, 3) * 3 * PL;
         for (int it = tid; it < (TY + 2 * PH) * (TX + 2 * PH); it += NT) {
           const int r = HH - PH + it / (TX + 2 * PH), c = 4 - PH + it % (TX + 2 * PH);
@@ -155,7 +159,7 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
           if (!(zg || i < 0 || i >= nx || j < 0 || j >= ny)) {
             const int o = r * W + c;
             if constexpr (F32) {
-              const Real h = -0.5f * kk;
+              const Real h = -0.5f * kk * ircp;  // the ring holds U = rho cp T
               f0 = (t0[o + 1] - t0[o - 1]) * (h * inv_len<Real, COORD, 0>(p.met, i, j, k));
               f1 = (t0[o + W] - t0[o - W]) * (h * inv_len<Real, COORD, 1>(p.met, i, j, k));
               f2 = (tp[o] - tm[o]) * (h * inv_len<Real, COORD, 2>(p.met, i, j, k));
