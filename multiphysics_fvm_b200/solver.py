@@ -7,15 +7,21 @@ copied to the host only at output steps (``n % output_frequency == 0``, after
 the step, labelled with the pre-step time as in src/solver.py:146-148).
 
 Extensions of the setup schema: ``time_config["n_steps"]`` (step-counted run,
-``t_end`` ignored), ``setup["precision"]`` ("fp32" | "fp64", default "fp64").
+``t_end`` ignored), ``setup["precision"]`` ("fp32" | "fp64", default "fp64"),
+``setup["restart_from"]`` (a snapshot written by ``io.save_snapshot`` through
+this loop: the state, its time and the step count are taken from it instead of
+the initial conditions; ``n_steps`` stays the total of the whole run, and the
+output steps and labels continue the numbering of the interrupted run).
 """
 from __future__ import annotations
 
+import inspect
 import math
 
 import numpy as np
 
 from . import backend
+from . import io
 from .grid import geometry
 
 
@@ -63,6 +69,20 @@ def _attach_closure(sim, spec):
     net.attach(sim, beta=float(spec.get("beta", 0.5)))
 
 
+def _advance(sim, k: int) -> int:
+    """Step up to ``k`` times; returns the steps taken (fewer once t > t_end)."""
+    before = sim.time()[1]
+    sim.step(k)
+    return sim.time()[1] - before
+
+
+def _accepts(fn, name: str) -> bool:
+    try:
+        return name in inspect.signature(fn).parameters
+    except (TypeError, ValueError):
+        return False
+
+
 def run(setup: dict, verbose: bool = True):
     """Run a setup (src/solver.py:88-151) with the state resident on the device.
     Returns the Simulation (its final state via ``download()``)."""
@@ -75,40 +95,47 @@ def run(setup: dict, verbose: bool = True):
     save = setup.get("save_config") or {}
     saver = save.get("saver")
     out_freq = int(save.get("output_frequency", 0) or 0)
-    grid = geometry.build_grid(setup["coordinate_system"], setup["grid_config"])
     U = physics.allocate_u(setup["grid_config"])
-    apply_ics(U, params, grid, setup["initial_conditions"])
+    n = 0
+    if setup.get("restart_from"):
+        t_start, n = io.restore_snapshot(setup["restart_from"], setup, U)
+    else:
+        grid = geometry.build_grid(setup["coordinate_system"], setup["grid_config"])
+        apply_ics(U, params, grid, setup["initial_conditions"])
     sim = backend.Simulation.from_setup(setup)
     sim.upload(U)
     sim.set_time(t_start, t_end, cfl)
     _attach_closure(sim, setup.get("closure"))
     limit = n_steps if n_steps is not None else None
-    n = 0
-    while True:
-        chunk = out_freq if out_freq > 0 else (limit if limit is not None else 1000)
-        if n == 0 and out_freq > 0:
-            chunk = 1
-        elif out_freq > 0:
-            chunk = out_freq - (n % out_freq) if n % out_freq else out_freq
+    takes_state_time = saver is not None and _accepts(saver, "state_time")
+    while limit is None or n < limit:
+        # Steps up to and including the next output step (step index k with
+        # k % out_freq == 0, i.e. the step after which n == k + 1).
+        if out_freq > 0:
+            chunk = (1 - n) % out_freq or out_freq
+        else:
+            chunk = 1000 if limit is None else limit - n
         if limit is not None:
             chunk = min(chunk, limit - n)
-            if chunk <= 0:
+        save_due = out_freq > 0 and (n + chunk - 1) % out_freq == 0
+        if save_due and chunk > 1:  # stop before the output step to read its start time
+            taken = _advance(sim, chunk - 1)
+            n += taken
+            if taken < chunk - 1:  # t passed t_end
                 break
-        t_before, n_before, _ = sim.time()
-        sim.step(chunk)
-        t, n_dev, dt = sim.time()
-        taken = n_dev - n_before
+            chunk = 1
+        t_pre = sim.time()[0]
+        taken = _advance(sim, chunk)
         n += taken
-        if taken == 0:
-            break
-        if out_freq > 0 and (n - 1) % out_freq == 0:
-            t_label = t - dt
+        if save_due and taken == chunk:
+            t, _, dt = sim.time()
             if verbose:
-                pct = 100 * t_label / t_end if math.isfinite(t_end) else 100 * n / max(limit or 1, 1)
-                print(f"n = {n - 1:6d} | t = {t_label:.2f}/{t_end:.2f} | dt = {dt:.2e} | {pct:.1f}%")
+                pct = 100 * t_pre / t_end if math.isfinite(t_end) else 100 * n / max(limit or 1, 1)
+                print(f"n = {n - 1:6d} | t = {t_pre:.2f}/{t_end:.2f} | dt = {dt:.2e} | {pct:.1f}%")
             if saver is not None:
                 sim.download_into(U)
-                saver(U, setup, t_label, n - 1, save.get("directory", "."))
+                extra = {"state_time": t} if takes_state_time else {}
+                saver(U, setup, t_pre, n - 1, save.get("directory", "."), **extra)
         if taken < chunk:  # t passed t_end inside the chunk
             break
     status = sim.status()
