@@ -370,7 +370,7 @@ cudaError_t launch_bc(fvm_handle* h, int b, bool use_active) {
 
 template <typename Real>
 cudaError_t launch_dt_reduce(fvm_handle* h) {
-  const int blocks = h->nsm * 4;
+  const int blocks = h->nsm * 3;  // the kernel's resident blocks per SM (__launch_bounds__)
   const Real* u = static_cast<const Real*>(h->U[0]);
   const double g = h->d.params[0], mu = h->d.params[1];
   switch (h->d.coords) {

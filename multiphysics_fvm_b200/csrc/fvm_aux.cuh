@@ -137,8 +137,9 @@ __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, co
                                                   double gam, double mu, Clock* clk, unsigned* status);
 
 template <typename Real, int COORD>
-__global__ void ns_dt_reduce_kernel(const Real* __restrict__ u, Layout L, Metric<double> m, double gam, double mu,
-                                    Clock* clk, unsigned* status) {
+__global__ void __launch_bounds__(256, 3)
+    ns_dt_reduce_kernel(const Real* __restrict__ u, Layout L, Metric<double> m, double gam, double mu, Clock* clk,
+                        unsigned* status) {
   ns_dt_reduce_body<Real, COORD>(u, L, m, gam, mu, clk, status);
 }
 
@@ -164,36 +165,53 @@ __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, co
   __shared__ double s_rc[32], s_nu[32];
   double rc = 0.0, nu = 0.0;
   unsigned bad = 0;
-  // one x1 row per block iteration, threads across the row: no 64-bit
-  // division per cell (rows = ny*nz < 2^31)
+  // x1 rows (rows = ny*nz < 2^31, no 64-bit division per cell), threads across
+  // the row.  Each thread first loads its cell of RB rows (RB*5 loads in
+  // flight) and then runs the float64 arithmetic, whose division and square
+  // root chains would otherwise leave the loads of one row exposed.
+  constexpr int RB = 4;
   const int rows = L.ny * L.nz;
-  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
-    const int j = row % L.ny, k = row / L.ny;
-    const long long g0 = L.idx(0, k + 1, j + 1, 1);
-   for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
-    const long long g = g0 + i;
-    // float64 throughout; one reciprocal of rho and the inverse-length tables
-    // replace the eight divisions (dt moves by ulps, inside the 1e-12 bound)
-    const double rho = double(u[g]);
-    const double ir = 1.0 / rho;
-    const double v0 = double(u[g + L.var_stride]) * ir, v1 = double(u[g + 2 * L.var_stride]) * ir,
-                 v2 = double(u[g + 3 * L.var_stride]) * ir;
-    const double E = double(u[g + 4 * L.var_stride]) * ir;
-    const double P = ((gam - 1.0) * rho) * (E - (((v0 * v0) + (v1 * v1)) + (v2 * v2)) / 2.0);
-    const double cs = sqrt((gam * P) * ir);
-    if (!(rho > 0.0)) bad |= ST_DENSITY;
-    if (!(P > 0.0)) bad |= ST_PRESSURE;
-    const double vv[3] = {v0, v1, v2};
-    double ml[3];
+  const int G = gridDim.x;
+  for (int row0 = blockIdx.x; row0 < rows; row0 += RB * G) {
+    for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
+      Real q[RB][5];
+      int jr[RB], kr[RB];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) ml[d] = fmax(fmax(fabs(vv[d] + 0.0), fabs(vv[d] + (-cs))), fabs(vv[d] + cs));
-    const double r = fmax(fmax(ml[0] * inv_len<double, COORD, 0>(m, i, j, k), ml[1] * inv_len<double, COORD, 1>(m, i, j, k)),
-                          ml[2] * inv_len<double, COORD, 2>(m, i, j, k));
-    const double nl = mu * ir;
-    if (!(r >= 0.0) || !(nl >= 0.0)) bad |= ST_NONFINITE;
-    rc = fmax(rc, r);
-    nu = fmax(nu, nl);
-   }
+      for (int b = 0; b < RB; ++b) {
+        const int row = row0 + b * G;
+        const bool in = row < rows;
+        jr[b] = in ? row % L.ny : 0;
+        kr[b] = in ? row / L.ny : 0;
+        const long long g = L.idx(0, kr[b] + 1, jr[b] + 1, 1) + i;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) q[b][v] = in ? u[g + v * L.var_stride] : Real(1);
+      }
+#pragma unroll
+      for (int b = 0; b < RB; ++b) {
+        if (row0 + b * G >= rows) continue;
+        const int j = jr[b], k = kr[b];
+        // float64 throughout; one reciprocal of rho and the inverse-length
+        // tables replace the eight divisions (dt moves by ulps, inside 1e-12)
+        const double rho = double(q[b][0]);
+        const double ir = 1.0 / rho;
+        const double v0 = double(q[b][1]) * ir, v1 = double(q[b][2]) * ir, v2 = double(q[b][3]) * ir;
+        const double E = double(q[b][4]) * ir;
+        const double P = ((gam - 1.0) * rho) * (E - (((v0 * v0) + (v1 * v1)) + (v2 * v2)) / 2.0);
+        const double cs = sqrt((gam * P) * ir);
+        if (!(rho > 0.0)) bad |= ST_DENSITY;
+        if (!(P > 0.0)) bad |= ST_PRESSURE;
+        const double vv[3] = {v0, v1, v2};
+        double ml[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) ml[d] = fmax(fmax(fabs(vv[d] + 0.0), fabs(vv[d] + (-cs))), fabs(vv[d] + cs));
+        const double r = fmax(fmax(ml[0] * inv_len<double, COORD, 0>(m, i, j, k), ml[1] * inv_len<double, COORD, 1>(m, i, j, k)),
+                              ml[2] * inv_len<double, COORD, 2>(m, i, j, k));
+        const double nl = mu * ir;
+        if (!(r >= 0.0) || !(nl >= 0.0)) bad |= ST_NONFINITE;
+        rc = fmax(rc, r);
+        nu = fmax(nu, nl);
+      }
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     rc = fmax(rc, __shfl_xor_sync(0xffffffffu, rc, o));

@@ -10,8 +10,10 @@
 //   D  Stokes stress on plane K+2, zero on ghosts     (viscous only, :102-142)
 //   E  x3 MUSCL slopes of cell K+1 for the block's columns (registers)
 //   F  x3 face flux at K+1/2 (registers; K-1/2 kept from the previous step)
-//   G  x1 and x2 slopes -> face states -> fluxes through shared memory,
-//      divergence, sources, stage combination, coalesced store of plane K.
+//   G  x1 slopes, face states and fluxes in registers (one warp per tile
+//      row, neighbours by shuffle); x2 slopes -> face states -> fluxes
+//      through shared memory; divergence, sources, stage combination,
+//      coalesced store of plane K.
 // HH = 3 with viscosity (tau at K+2 needs v at K+3), 2 without.
 #pragma once
 #include "fvm_common.cuh"
@@ -96,7 +98,11 @@ struct NsCfg {
   static constexpr int OFF_T = OFF_P + 3 * PL2;
   static constexpr int OFF_S = OFF_T + (VISC ? 3 * 6 * PL2 : 0);
   static constexpr int OFF_FB = OFF_S + NREC * XB;
-  static constexpr int END = OFF_FB + 5 * FB;
+  // x1 halo data per plane parity: slopes of the cell left of the tile (per
+  // field and row) and fluxes through the tile's right edge (per row)
+  static constexpr int OFF_HL = OFF_FB + 5 * FB;
+  static constexpr int OFF_FR = OFF_HL + 2 * NREC * TY;
+  static constexpr int END = OFF_FR + 2 * 5 * TY;
   static constexpr int BYTES = round_up(END * (int)sizeof(Real), 16) + NSLOT * 8;
   static constexpr unsigned TX_BYTES = NV * PL * sizeof(Real);
 };
@@ -179,6 +185,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
   Real* tring = sm + C::OFF_T;
   Real* sl = sm + C::OFF_S;
   Real* fb = sm + C::OFF_FB;
+  Real* hl = sm + C::OFF_HL;
+  Real* fr = sm + C::OFF_FR;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (C::BYTES - C::NSLOT * 8));
 
   if (smem_u32(smem_raw) & 127u) {  // TMA destinations need 128-byte alignment
@@ -446,63 +454,99 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
 #pragma unroll
         for (int f = 0; f < NREC; ++f) zs[f] = zn[f];
       }
-      if (K < Z0) { __syncthreads(); continue; }
-      const int kK = K - 1;  // interior index of the output plane
-      // ------------------------------------------------ G: x1 slopes ----
-      // Task maps of the x1 phases: warp w < TY takes the 32 cells (faces) of
-      // row w, the two spare warps the row ends, so no warp straddles two ring
-      // rows (whose 40-float stride would put lanes on the same bank).
+      // ------------------------------------------------------ x1 halo ----
+      // While the output warps run E and F, the spare warps form the x1 halo
+      // data of plane Kh (the next output plane; on a flat grid this one):
+      // the first spare warp the slopes of the cell left of the tile, the
+      // second the flux through the tile's right edge, one lane per row.
       {
-        constexpr int ti[3] = {0, 3, 4};  // tau row 1 = (t11, t12, t13)
-        const int hh = tid - TX * TY;     // halo task of a spare-warp thread
-        if (is_out || hh < 2 * TY) {
-          const int ty = is_out ? oty : hh >> 1, tx = is_out ? otx : ((hh & 1) ? TX : -1);
-          const int it = ty * (TX + 2) + tx + 1;
-          const int i = x0 + tx, j = y0 + ty;
-          const bool interior = i >= 0 && i < nx && j < ny;
-          const Real l1 = (F32 || !interior) ? Real(1) : G::L1(p.met, i, j, kK);
+        const int Kh = flat ? K : K + 1;
+        const int hh = tid - TX * TY, row = hh & 31;
+        if (!is_out && row < TY && Kh >= Z0 && Kh <= Zl) {
+          constexpr int ti[3] = {0, 3, 4};  // tau row 1 = (t11, t12, t13)
+          const Real* uh = uring + pmod(Kh, C::NSLOT) * C::SLOT;
+          const Real* ph = pring + pmod(Kh, 3) * PL2;
+          const Real* th = tring + pmod(Kh, 3) * 6 * PL2;
+          const int kh = Kh - 1, j = y0 + row, par = Kh & 1;
+          if (hh < 32) {
+            const int i = x0 - 1;
+            const bool in = i >= 0 && j < ny;  // i < nx as x0 < nx
+            const Real l1 = (F32 || !in) ? Real(1) : G::L1(p.met, i, j, kh);
 #pragma unroll
-          for (int f = 0; f < NREC; ++f) {
-            const Real s = interior ? muscl_slope<LIM>(field(uK, pK, tK, ti, f, tx - 1, ty), field(uK, pK, tK, ti, f, tx, ty),
-                                                       field(uK, pK, tK, ti, f, tx + 1, ty), l1)
-                                    : Real(0);
-            sl[f * C::XB + it] = s;
-          }
-        }
-      }
-      __syncthreads();
-      {
-        constexpr int ti[3] = {0, 3, 4};
-        const int hh = tid - TX * TY;
-        if (is_out || hh < TY) {
-          const int ty = is_out ? oty : hh, fx = is_out ? otx : TX;
-          const int it = ty * (TX + 1) + fx;
-          const int fi = x0 + fx, j = y0 + ty;
-          Real F[5] = {Real(0), Real(0), Real(0), Real(0), Real(0)};
-          if (fi <= nx && j < ny) {
-            Real qL[NREC], qR[NREC];
-            const int oL = ty * (TX + 2) + fx;  // slope slot of the left cell (tx = fx-1)
+            for (int f = 0; f < NREC; ++f)
+              hl[(par * NREC + f) * TY + row] =
+                  in ? muscl_slope<LIM>(field(uh, ph, th, ti, f, -2, row), field(uh, ph, th, ti, f, -1, row),
+                                        field(uh, ph, th, ti, f, 0, row), l1)
+                     : Real(0);
+          } else {
+            const int i = x0 + TX;  // face between cells i-1 and i
+            Real F[5] = {Real(0), Real(0), Real(0), Real(0), Real(0)};
+            if (i <= nx && j < ny) {
+              const bool in0 = i < nx;  // cell i-1 is interior here
+              const Real l1m = F32 ? Real(1) : G::L1(p.met, i - 1, j, kh);
+              const Real l1 = (F32 || !in0) ? Real(1) : G::L1(p.met, i, j, kh);
+              Real qL[NREC], qR[NREC];
 #pragma unroll
-            for (int f = 0; f < NREC; ++f) {
-              qL[f] = field(uK, pK, tK, ti, f, fx - 1, ty) + sl[f * C::XB + oL] / Real(2);
-              qR[f] = field(uK, pK, tK, ti, f, fx, ty) - sl[f * C::XB + oL + 1] / Real(2);
+              for (int f = 0; f < NREC; ++f) {
+                const Real fa = field(uh, ph, th, ti, f, TX - 2, row), fb1 = field(uh, ph, th, ti, f, TX - 1, row);
+                const Real fc = field(uh, ph, th, ti, f, TX, row), fd = field(uh, ph, th, ti, f, TX + 1, row);
+                const Real sm1 = muscl_slope<LIM>(fa, fb1, fc, l1m);
+                const Real s0 = in0 ? muscl_slope<LIM>(fb1, fc, fd, l1) : Real(0);
+                qL[f] = fb1 + sm1 / Real(2);
+                qR[f] = fc - s0 / Real(2);
+              }
+              ns_flux<Real, 0, RIEM, VISC>(qL, qR, gam, F);
+              const Real s1 = G::S1(p.met, i, j, kh);
+#pragma unroll
+              for (int v = 0; v < 5; ++v) F[v] = F[v] * s1;
             }
-            ns_flux<Real, 0, RIEM, VISC>(qL, qR, gam, F);
-            const Real s1 = G::S1(p.met, fi, j, kK);
 #pragma unroll
-            for (int v = 0; v < 5; ++v) F[v] = F[v] * s1;
+            for (int v = 0; v < 5; ++v) fr[(par * 5 + v) * TY + row] = F[v];
           }
-#pragma unroll
-          for (int v = 0; v < 5; ++v) fb[v * C::FB + it] = F[v];
         }
       }
-      __syncthreads();
+      if (K < Z0) { __syncthreads(); continue; }
+      if (flat) __syncthreads();  // a flat grid's halo data is this step's
+      const int kK = K - 1;  // interior index of the output plane
+      // ------------------------------------------------------ G: x1 ----
+      // Warp w < TY owns tile row w.  Each lane forms the x1 slopes of its
+      // cell and the flux through the cell's left face in registers; the left
+      // cell's slope comes from the previous lane (shuffle) and, for lane 0,
+      // from the halo data.  The right-face flux is the next lane's left-face
+      // flux and, for lane 31, the halo flux through the tile's right edge.
+      // Each face's arithmetic is that of a slopes-then-faces pass, so the
+      // results are the same.
       Real Fxm[5], Fxp[5];
       if (is_out) {
+        constexpr int ti[3] = {0, 3, 4};  // tau row 1 = (t11, t12, t13)
+        const int tx = otx, ty = oty, par = K & 1;
+        const int i = x0 + tx, j = y0 + ty;
+        const bool in0 = i < nx && j < ny;  // this cell (i >= 0)
+        const Real l1 = (F32 || !in0) ? Real(1) : G::L1(p.met, i, j, kK);
+        Real qL[NREC], qR[NREC];
+#pragma unroll
+        for (int f = 0; f < NREC; ++f) {
+          const Real fm = field(uK, pK, tK, ti, f, tx - 1, ty);
+          const Real f0 = field(uK, pK, tK, ti, f, tx, ty);
+          const Real s0 = in0 ? muscl_slope<LIM>(fm, f0, field(uK, pK, tK, ti, f, tx + 1, ty), l1) : Real(0);
+          const Real su = __shfl_up_sync(0xffffffffu, s0, 1);
+          const Real sh = hl[(par * NREC + f) * TY + ty];
+          qL[f] = fm + (tx == 0 ? sh : su) / Real(2);
+          qR[f] = f0 - s0 / Real(2);
+        }
+        Real F[5] = {Real(0), Real(0), Real(0), Real(0), Real(0)};
+        if (i <= nx && j < ny) {  // face i, between cells i-1 and i
+          ns_flux<Real, 0, RIEM, VISC>(qL, qR, gam, F);
+          const Real s1 = G::S1(p.met, i, j, kK);
+#pragma unroll
+          for (int v = 0; v < 5; ++v) F[v] = F[v] * s1;
+        }
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          Fxm[v] = fb[v * C::FB + oty * (TX + 1) + otx];
-          Fxp[v] = fb[v * C::FB + oty * (TX + 1) + otx + 1];
+          Fxm[v] = F[v];
+          const Real fd = __shfl_down_sync(0xffffffffu, F[v], 1);
+          const Real fe = fr[(par * 5 + v) * TY + ty];
+          Fxp[v] = tx == TX - 1 ? fe : fd;
         }
       }
       // ------------------------------------------------ G: x2 slopes ----

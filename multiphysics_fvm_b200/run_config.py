@@ -71,6 +71,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--precision", default=None)
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--breakdown", action="store_true",
+                    help="also time each launch of a few un-captured steps: stage kernels vs the rest")
     a = ap.parse_args()
     if a.config == "batch_c3":
         run_batch(a.steps, a.warmup, a.autotune)
@@ -85,6 +87,10 @@ def main():
     if tuned:
         print(f"autotuned tile rows {sim.tiling()[0]}, z-march depth {tuned[0]} ({tuned[1]:.3f} ms/step in the sweep)")
     print(f"{a.config} n={a.n} {s.get('precision')}: {ms / a.steps:.3f} ms/step, status={sim.status()}")
+    if a.breakdown:
+        n = max(3, min(a.steps, 10))
+        st, ot, nl = sim.profile_steps(n)
+        print(f"  per step: stage kernels {st / n:.3f} ms ({nl // n} launches), other kernels {ot / n:.3f} ms")
 
 
 if __name__ == "__main__":
