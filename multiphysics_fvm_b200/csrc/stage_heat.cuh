@@ -128,6 +128,14 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         phase_bits ^= 1u << s;
         pending &= ~(1u << s);
       }
+      // U0 and acc of this plane's output cell, loaded now so that the rest
+      // of the step hides their latency
+      Real eu0 = Real(0), eacc = Real(0);
+      if (K >= Z0 && out_valid) {
+        const long long g0 = L.idx(0, K, oj + 1, oi + 1);
+        if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) eu0 = p.u0[g0];
+        if (needs_acc(p.coef)) eacc = p.acc[g0];
+      }
       // T on the newest plane (heat.py:74).  T = U / (rho cp) is linear in U,
       // so the float32 path differences the U ring directly and folds
       // 1/(rho cp) into the gradient factor (no T ring, no barrier); float64
@@ -213,9 +221,7 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
           else k = (-sum) / G::V(p.met, oi, oj, kK) + qsrc;
           const long long gi = L.idx(0, K, oj + 1, oi + 1);
           const Real ucur = U(K, oty + HH, otx + 4);
-          Real u0v = Real(0), accv = Real(0);
-          if (needs_u0<Real>(p.coef)) u0v = p.coef.u0_is_input ? ucur : p.u0[gi];
-          if (needs_acc(p.coef)) accv = p.acc[gi];
+          const Real u0v = (needs_u0<Real>(p.coef) && p.coef.u0_is_input) ? ucur : eu0, accv = eacc;
           const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
           p.out[gi] = o;
           if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
@@ -223,11 +229,6 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         }
         __syncthreads();
         continue;
-      }
-      if (out_valid && otx == 0) {
-        const long long g0 = L.idx(0, K, oj + 1, oi + 1);
-        if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0);
-        if (needs_acc(p.coef)) prefetch_l2(p.acc + g0);
       }
       // x1 faces of plane K
       for (int it = tid; it < TY * (TX + 2); it += NT) {
@@ -287,9 +288,7 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         else k = (-sum) / G::V(p.met, oi, oj, kK) + qsrc;
         const long long gi = L.idx(0, K, oj + 1, oi + 1);
         const Real ucur = U(K, oty + HH, otx + 4);
-        Real u0v = Real(0), accv = Real(0);
-        if (needs_u0<Real>(p.coef)) u0v = p.coef.u0_is_input ? ucur : p.u0[gi];
-        if (needs_acc(p.coef)) accv = p.acc[gi];
+        const Real u0v = (needs_u0<Real>(p.coef) && p.coef.u0_is_input) ? ucur : eu0, accv = eacc;
         const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
         p.out[gi] = o;
         if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);

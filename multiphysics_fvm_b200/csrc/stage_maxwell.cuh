@@ -392,22 +392,33 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
         }
         const Real Vc = G::V(p.met, oi, oj, kK);
         const long long gidx = L.idx(0, K, oj + 1, oi + 1);
-        unsigned bad = 0;
+        // residual of each variable first (the flux registers die), then
+        // every global load of the cell before its first store: the stores
+        // may alias later loads as far as the compiler knows, which would
+        // otherwise cost one memory round trip per variable
+        Real kv[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const Real Fym = fb[v * C::FB + oty * TX + otx], Fyp = fb[v * C::FB + (oty + 1) * TX + otx];
           const Real sum = ((((Fxp[v] - Fxm[v]) + Fyp) - Fym) + Fzn[v]) - Fzp[v];
           const Real sp = v < 3 ? Real(0) : (-Real(p.sigma)) * (q[v] / ep);
-          Real k;
-          if constexpr (sizeof(Real) == 4) k = (-sum) * rcp_approx(Vc) + ((sg[v] + sp) + sc[v]);
-          else k = (-sum) / Vc + ((sg[v] + sp) + sc[v]);
+          if constexpr (sizeof(Real) == 4) kv[v] = (-sum) * rcp_approx(Vc) + ((sg[v] + sp) + sc[v]);
+          else kv[v] = (-sum) / Vc + ((sg[v] + sp) + sc[v]);
+        }
+        Real u0v[NV], accv[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
           const long long gi = gidx + (long long)v * L.var_stride;
-          Real u0v = Real(0), accv = Real(0);
-          if (needs_u0<Real>(p.coef)) u0v = p.coef.u0_is_input ? q[v] : p.u0[gi];
-          if (needs_acc(p.coef)) accv = p.acc[gi];
-          const Real o = stage_combine(p.coef, dt, k, q[v], u0v, accv);
+          u0v[v] = needs_u0<Real>(p.coef) ? (p.coef.u0_is_input ? q[v] : p.u0[gi]) : Real(0);
+          accv[v] = needs_acc(p.coef) ? p.acc[gi] : Real(0);
+        }
+        unsigned bad = 0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const long long gi = gidx + (long long)v * L.var_stride;
+          const Real o = stage_combine(p.coef, dt, kv[v], q[v], u0v[v], accv[v]);
           p.out[gi] = o;
-          if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
+          if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, kv[v], u0v[v], accv[v]);
           if (!isfinite(o)) bad |= ST_NONFINITE;
         }
         if (bad) atomicOr(p.status, bad);

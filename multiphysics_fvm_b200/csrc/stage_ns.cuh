@@ -177,6 +177,9 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
   constexpr int TX = C::TX, NT = C::NT, W = C::W, PL = C::PL, HH = C::HH, NREC = C::NREC;
   constexpr int W2 = C::W2, PL2 = C::PL2;
   constexpr bool F32 = sizeof(Real) == 4;
+  // load U0/acc at the start of each step where registers permit (the
+  // inviscid kernels, 320 threads per block, would spill)
+  constexpr bool EARLY = VISC;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Real* sm = reinterpret_cast<Real*>(smem_raw);
   Real* uring = sm + C::OFF_U;
@@ -289,12 +292,26 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       const Real* tK = tring + pmod(K, 3) * 6 * PL2;
       const Real* tK1 = tring + pmod(K + 1, 3) * 6 * PL2;
       const Real* tK2 = tring + pmod(K + 2, 3) * 6 * PL2;
-      // lane 0 of each output row asks L2 for this plane's U0/acc rows
-      if (K >= Z0 && out_valid && otx == 0) {
+      // U0 and acc of this plane's output cells.  With registers to spare
+      // (EARLY) each output thread loads them here, so that the whole step
+      // hides their latency; otherwise lane 0 of each output row asks L2 for
+      // the rows and the output phase loads them.
+      Real eu0[5], eacc[5];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) { eu0[v] = Real(0); eacc[v] = Real(0); }
+      if (K >= Z0 && out_valid) {
         const long long g0 = L.idx(0, K, oj + 1, oi + 1);
-        for (int v = 0; v < 5; ++v) {
-          if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
-          if (needs_acc(p.coef)) prefetch_l2(p.acc + g0 + v * L.var_stride);
+        if constexpr (EARLY) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) {
+            if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) eu0[v] = p.u0[g0 + v * L.var_stride];
+            if (needs_acc(p.coef)) eacc[v] = p.acc[g0 + v * L.var_stride];
+          }
+        } else if (otx == 0) {
+          for (int v = 0; v < 5; ++v) {
+            if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
+            if (needs_acc(p.coef)) prefetch_l2(p.acc + g0 + v * L.var_stride);
+          }
         }
       }
       // ---------------------------------------------------------- B ----
@@ -651,22 +668,38 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         const Real Vc = G::V(p.met, oi, oj, kK);
         const Real iV = recip(Vc);
         const long long gidx = L.idx(0, K, oj + 1, oi + 1);
-        unsigned bad = 0;
+        // residual of each variable first (the flux registers die), then
+        // every global load of the cell before its first store: the stores
+        // may alias later loads as far as the compiler knows, which would
+        // otherwise cost one memory round trip per variable
+        Real kv[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
           const Real Fym = fb[v * C::FB + oty * TX + otx];
           const Real Fyp = fb[v * C::FB + (oty + 1) * TX + otx];
           const Real sum = ((((Fxp[v] - Fxm[v]) + Fyp) - Fym) + Fzn[v]) - Fzp[v];
-          Real k;
-          if constexpr (F32) k = (-sum) * iV + src[v];
-          else k = (-sum) / Vc + src[v];
+          if constexpr (F32) kv[v] = (-sum) * iV + src[v];
+          else kv[v] = (-sum) / Vc + src[v];
+        }
+        Real u0v[5], accv[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
           const long long gi = gidx + (long long)v * L.var_stride;
-          Real u0v = Real(0), accv = Real(0);
-          if (needs_u0<Real>(p.coef)) u0v = p.coef.u0_is_input ? q[v] : p.u0[gi];
-          if (needs_acc(p.coef)) accv = p.acc[gi];
-          const Real o = stage_combine(p.coef, dt, k, q[v], u0v, accv);
+          if constexpr (EARLY) {
+            u0v[v] = (needs_u0<Real>(p.coef) && p.coef.u0_is_input) ? q[v] : eu0[v];
+            accv[v] = eacc[v];
+          } else {
+            u0v[v] = needs_u0<Real>(p.coef) ? (p.coef.u0_is_input ? q[v] : p.u0[gi]) : Real(0);
+            accv[v] = needs_acc(p.coef) ? p.acc[gi] : Real(0);
+          }
+        }
+        unsigned bad = 0;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const long long gi = gidx + (long long)v * L.var_stride;
+          const Real o = stage_combine(p.coef, dt, kv[v], q[v], u0v[v], accv[v]);
           p.out[gi] = o;
-          if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
+          if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, kv[v], u0v[v], accv[v]);
           if (!isfinite(o)) bad |= ST_NONFINITE;
           if (v == 0 && p.coef.mode != MODE_RHS && !(o > Real(0))) bad |= ST_DENSITY;
         }
