@@ -308,6 +308,12 @@ struct StageCoef {
 __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
+// One 4-byte asynchronous copy global -> shared (completion: cp_async_wait_all
+// by the issuing thread, after which the thread may read the destination).
+__device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Combine one variable.  `k` is the residual, `ucur` the stage input, `u0`
 // the step's base state, `acc` the running k-sum.  Op order follows

@@ -48,7 +48,13 @@ struct MaxwellCfg {
   static constexpr int OFF_FL = OFF_R + 3 * 2 * PL;
   static constexpr int OFF_FR = OFF_FL + NV * XB;
   static constexpr int OFF_FB = OFF_FR + NV * XB;
-  static constexpr int END = OFF_FB + NV * FB;
+  // U0 and acc of the plane's output cells copied in by cp.async at the start
+  // of each step ([U0 | acc][variable][output thread]).  Off: with the extra
+  // 9 KB per block the three float32 blocks per SM leave too little L1 for
+  // the metric tables, and the step was slower (2.48 -> 2.53 ms on C2a).
+  static constexpr bool STAGED = false;
+  static constexpr int OFF_G = OFF_FB + NV * FB;
+  static constexpr int END = OFF_G + (STAGED ? 2 * NV * TX * TY : 0);
   static constexpr int BYTES = round_up(END * (int)sizeof(Real), 16) + NSLOT * 8;
   static constexpr unsigned TX_BYTES = NV * PL * sizeof(Real);
 };
@@ -111,6 +117,9 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
   Real* fL = sm + C::OFF_FL;
   Real* fR = sm + C::OFF_FR;
   Real* fb = sm + C::OFF_FB;
+  Real* gst = sm + C::OFF_G;
+  constexpr bool STAGED = C::STAGED;
+  constexpr int NO = TX * TY;  // output threads
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (C::BYTES - C::NSLOT * 8));
   if (p.active && !*p.active) return;
   if (smem_u32(smem_raw) & 127u) {
@@ -167,6 +176,24 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
         }
         phase_bits ^= 1u << s;
         pending &= ~(1u << s);
+      }
+      // U0 and acc of this plane's output cells, fetched now so that the
+      // step hides their latency: copied into this thread's shared-memory
+      // slots (STAGED), or lane 0 of each row asks L2 for them
+      if (K >= Z0 && out_valid) {
+        const long long g0 = L.idx(0, K, oj + 1, oi + 1);
+        if constexpr (STAGED) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) cp_async4(&gst[v * NO + tid], p.u0 + g0 + v * L.var_stride);
+            if (needs_acc(p.coef)) cp_async4(&gst[(NV + v) * NO + tid], p.acc + g0 + v * L.var_stride);
+          }
+        } else if (otx == 0) {
+          for (int v = 0; v < NV; ++v) {
+            if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
+            if (needs_acc(p.coef)) prefetch_l2(p.acc + g0 + v * L.var_stride);
+          }
+        }
       }
       const Real* uK = uring + pmod(K, C::NSLOT) * C::SLOT;
       const Real* uK1 = uring + pmod(K + 1, C::NSLOT) * C::SLOT;
@@ -247,13 +274,6 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
       __syncthreads();
       if (K < Z0) continue;
       const int kK = K - 1;
-      if (out_valid && otx == 0) {
-        const long long g0 = L.idx(0, K, oj + 1, oi + 1);
-        for (int v = 0; v < NV; ++v) {
-          if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) prefetch_l2(p.u0 + g0 + v * L.var_stride);
-          if (needs_acc(p.coef)) prefetch_l2(p.acc + g0 + v * L.var_stride);
-        }
-      }
       // x1 faces
       for (int it = tid; it < TY * (TX + 2); it += NT) {
         const int ty = it / (TX + 2), tx = it % (TX + 2) - 1;
@@ -406,11 +426,17 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
           else kv[v] = (-sum) / Vc + ((sg[v] + sp) + sc[v]);
         }
         Real u0v[NV], accv[NV];
+        if constexpr (STAGED) cp_async_wait_all();
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const long long gi = gidx + (long long)v * L.var_stride;
-          u0v[v] = needs_u0<Real>(p.coef) ? (p.coef.u0_is_input ? q[v] : p.u0[gi]) : Real(0);
-          accv[v] = needs_acc(p.coef) ? p.acc[gi] : Real(0);
+          if constexpr (STAGED) {
+            u0v[v] = needs_u0<Real>(p.coef) ? (p.coef.u0_is_input ? q[v] : gst[v * NO + tid]) : Real(0);
+            accv[v] = needs_acc(p.coef) ? gst[(NV + v) * NO + tid] : Real(0);
+          } else {
+            u0v[v] = needs_u0<Real>(p.coef) ? (p.coef.u0_is_input ? q[v] : p.u0[gi]) : Real(0);
+            accv[v] = needs_acc(p.coef) ? p.acc[gi] : Real(0);
+          }
         }
         unsigned bad = 0;
 #pragma unroll
@@ -426,6 +452,7 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
       __syncthreads();
     }
   }
+  if constexpr (STAGED) cp_async_wait_all();  // none left in flight at exit
   if (!ok && tid == 0)
     for (int s = 0; s < C::NSLOT; ++s)
       if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 1000000000ull);

@@ -102,7 +102,11 @@ struct NsCfg {
   // field and row) and fluxes through the tile's right edge (per row)
   static constexpr int OFF_HL = OFF_FB + 5 * FB;
   static constexpr int OFF_FR = OFF_HL + 2 * NREC * TY;
-  static constexpr int END = OFF_FR + 2 * 5 * TY;
+  // float32 inviscid: U0 and acc of the plane's output cells, copied in by
+  // cp.async at the start of each step ([U0 | acc][variable][output thread])
+  static constexpr bool STAGED = sizeof(Real) == 4 && !VISC;
+  static constexpr int OFF_G = OFF_FR + 2 * 5 * TY;
+  static constexpr int END = OFF_G + (STAGED ? 2 * 5 * TX * TY : 0);
   static constexpr int BYTES = round_up(END * (int)sizeof(Real), 16) + NSLOT * 8;
   static constexpr unsigned TX_BYTES = NV * PL * sizeof(Real);
 };
@@ -177,9 +181,12 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
   constexpr int TX = C::TX, NT = C::NT, W = C::W, PL = C::PL, HH = C::HH, NREC = C::NREC;
   constexpr int W2 = C::W2, PL2 = C::PL2;
   constexpr bool F32 = sizeof(Real) == 4;
-  // load U0/acc at the start of each step where registers permit (the
-  // inviscid kernels, 320 threads per block, would spill)
+  // U0/acc of each step's output cells: loaded into registers at the start of
+  // the step where registers permit (EARLY); the float32 inviscid kernels (64
+  // registers) copy them into shared memory instead (C::STAGED)
   constexpr bool EARLY = VISC;
+  constexpr bool STAGED = C::STAGED;
+  constexpr int NO = TX * TY;  // output threads
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Real* sm = reinterpret_cast<Real*>(smem_raw);
   Real* uring = sm + C::OFF_U;
@@ -190,6 +197,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
   Real* fb = sm + C::OFF_FB;
   Real* hl = sm + C::OFF_HL;
   Real* fr = sm + C::OFF_FR;
+  Real* gst = sm + C::OFF_G;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (C::BYTES - C::NSLOT * 8));
 
   if (smem_u32(smem_raw) & 127u) {  // TMA destinations need 128-byte alignment
@@ -292,10 +300,10 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       const Real* tK = tring + pmod(K, 3) * 6 * PL2;
       const Real* tK1 = tring + pmod(K + 1, 3) * 6 * PL2;
       const Real* tK2 = tring + pmod(K + 2, 3) * 6 * PL2;
-      // U0 and acc of this plane's output cells.  With registers to spare
-      // (EARLY) each output thread loads them here, so that the whole step
-      // hides their latency; otherwise lane 0 of each output row asks L2 for
-      // the rows and the output phase loads them.
+      // U0 and acc of this plane's output cells, fetched here so that the
+      // whole step hides their latency: into registers (EARLY), into this
+      // thread's shared-memory slots (STAGED), or else lane 0 of each output
+      // row asks L2 for the rows and the output phase loads them.
       Real eu0[5], eacc[5];
 #pragma unroll
       for (int v = 0; v < 5; ++v) { eu0[v] = Real(0); eacc[v] = Real(0); }
@@ -306,6 +314,12 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
           for (int v = 0; v < 5; ++v) {
             if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) eu0[v] = p.u0[g0 + v * L.var_stride];
             if (needs_acc(p.coef)) eacc[v] = p.acc[g0 + v * L.var_stride];
+          }
+        } else if constexpr (STAGED) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) {
+            if (needs_u0<Real>(p.coef) && !p.coef.u0_is_input) cp_async4(&gst[v * NO + tid], p.u0 + g0 + v * L.var_stride);
+            if (needs_acc(p.coef)) cp_async4(&gst[(5 + v) * NO + tid], p.acc + g0 + v * L.var_stride);
           }
         } else if (otx == 0) {
           for (int v = 0; v < 5; ++v) {
@@ -682,10 +696,14 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
           else kv[v] = (-sum) / Vc + src[v];
         }
         Real u0v[5], accv[5];
+        if constexpr (STAGED) cp_async_wait_all();
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
           const long long gi = gidx + (long long)v * L.var_stride;
-          if constexpr (EARLY) {
+          if constexpr (STAGED) {
+            u0v[v] = needs_u0<Real>(p.coef) ? (p.coef.u0_is_input ? q[v] : gst[v * NO + tid]) : Real(0);
+            accv[v] = needs_acc(p.coef) ? gst[(5 + v) * NO + tid] : Real(0);
+          } else if constexpr (EARLY) {
             u0v[v] = (needs_u0<Real>(p.coef) && p.coef.u0_is_input) ? q[v] : eu0[v];
             accv[v] = eacc[v];
           } else {
@@ -708,6 +726,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       __syncthreads();
     }
   }
+  if constexpr (STAGED) cp_async_wait_all();  // none left in flight at exit
   // On a timeout, wait (bounded) for every load this block may still have in flight.
   if (!ok && tid == 0) {
     for (int s = 0; s < C::NSLOT; ++s)
