@@ -359,12 +359,11 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
 
 cudaError_t launch_bc(fvm_handle* h, int b, bool use_active) {
   const Layout& L = h->lay;
-  const long long work = 2ll * h->nv * ((long long)L.ny * L.nz + (long long)L.nx * L.nz + (long long)L.nx * L.ny);
-  int blocks = (int)std::min<long long>((work + 255) / 256, 4096);
+  const dim3 grid((unsigned)std::min(std::max(L.nz, L.ny), 4096), (unsigned)(6 * h->nv));
   const BcSpec bc = make_bc(h->d, h->nv);
   const int* act = use_active ? &h->clk->active : nullptr;
-  if (h->f64) bc_fill_kernel<double><<<blocks, 256, 0, h->stream>>>(static_cast<double*>(h->U[b]), L, h->nv, bc, act);
-  else bc_fill_kernel<float><<<blocks, 256, 0, h->stream>>>(static_cast<float*>(h->U[b]), L, h->nv, bc, act);
+  if (h->f64) bc_fill_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<double*>(h->U[b]), L, h->nv, bc, act);
+  else bc_fill_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<float*>(h->U[b]), L, h->nv, bc, act);
   return cudaGetLastError();
 }
 

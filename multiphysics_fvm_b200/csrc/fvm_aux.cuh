@@ -49,18 +49,32 @@ __device__ __forceinline__ void bc_fill_one(Real* __restrict__ u, const Layout& 
   }
 }
 
+// One grid's ghost faces: blockIdx.y = variable * 6 + side, blocks over the
+// face's rows b, threads along a row a (the (a, b) of bc_fill_one), so no
+// index is decoded by division.
 template <typename Real>
 __global__ void bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc, const int* active) {
   if (active && !*active) return;
-  const long long total = bc_face_count(L, nv);
-  if (total < 0x7fffffffll) {
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < (int)total; t += gridDim.x * blockDim.x)
-      bc_fill_one<Real, int>(u, L, bc, t);
-  } else {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x)
-      bc_fill_one<Real, long long>(u, L, bc, t);
-  }
+  const int q = blockIdx.y / 6, side = blockIdx.y % 6;
+  if (q >= nv) return;
+  const int axis = side >> 1, high = side & 1;
+  const int A = axis == 0 ? L.ny : L.nx;  // along a row
+  const int B = axis == 2 ? L.ny : L.nz;  // rows
+  const int kind = bc.kind[q][side];
+  const int n = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
+  const int g = high ? n + 1 : 0;                       // ghost index along axis
+  const int inner = high ? n : 1;                       // adjacent interior
+  const int src = kind == 0 ? (high ? 1 : n) : inner;  // periodic: opposite layer
+  const Real two_w = Real(2) * Real(bc.value[q][side]);
+  for (int b = blockIdx.x; b < B; b += gridDim.x)
+    for (int a = threadIdx.x; a < A; a += blockDim.x) {
+      long long gi, si;
+      if (axis == 0) { gi = L.idx(q, b + 1, a + 1, g); si = L.idx(q, b + 1, a + 1, src); }
+      else if (axis == 1) { gi = L.idx(q, b + 1, g, a + 1); si = L.idx(q, b + 1, src, a + 1); }
+      else { gi = L.idx(q, g, b + 1, a + 1); si = L.idx(q, src, b + 1, a + 1); }
+      const Real v = u[si];
+      u[gi] = kind == 2 ? -v : (kind == 3 ? two_w - v : v);
+    }
 }
 
 // Reference layout (C order, last axis fastest) <-> device layout (x1 fastest).
