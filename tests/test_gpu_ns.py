@@ -142,6 +142,37 @@ def test_kh_multistep_fp64_and_fp32():
         sim.close()
 
 
+@pytest.mark.parametrize("ybc", ["periodic", "walls"])
+def test_flat_grid_partial_tiles_fp32(ybc):
+    """A one-plane float32 inviscid grid skips the x3 pipeline ("flat") and forms
+    its x1 halo data (the slope left of each tile, the flux through its right
+    edge) within the step.  45 x 27 x 1 leaves partial tiles in x and y; with
+    walls, x2 is reflecting for momentum_x2 and Neumann for the rest.  50 SSPRK3
+    steps with the device CFL dt against the oracle: relative L2 <= 1e-4."""
+    from multiphysics_fvm_b200.backend import Simulation
+    s, U = _kh_state((45, 27, 1), seed=4)
+    kinds = [["periodic"] * 6 for _ in range(5)]
+    if ybc == "walls":
+        for q in range(5):
+            kinds[q][2] = kinds[q][3] = "reflecting" if q == 2 else "neumann"
+    s["boundary_conditions"] = bcs_dict("navier_stokes", kinds)
+    geo = O.Geometry("cartesian", s["grid_config"])
+    Uo = U.copy()
+    dts = O.run("navier_stokes", Uo, s["physical_parameters"], geo,
+                dict(reconstructor="muscl", slope_limiter="minmod", riemann_solver="hll"), oracle_bcs(kinds),
+                "rk3_ssp", 0.4, 50)
+    s["precision"] = "fp32"
+    sim = Simulation.from_setup(s)
+    sim.upload(U)
+    sim.set_time(0.0, float("inf"), 0.4)
+    sim.step(50)
+    t, n, _ = sim.time()
+    assert n == 50 and sim.status() == 0
+    assert abs(t - sum(dts)) <= 1e-5 * sum(dts)
+    assert rel_l2(sim.download()[I3], Uo[I3]) <= 1e-4
+    sim.close()
+
+
 def test_conservation_periodic_pc_3d_fp32():
     """Piecewise-constant reconstruction in a triply periodic box: both copies of
     every boundary face see the same states, so mass, momentum and energy are
