@@ -272,7 +272,6 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
 
     for (int K = Kfirst; K <= Zl; ++K) {
       // ---------------------------------------------------------- A ----
-      if (tid == 0 && K > Kfirst && K + HH + 1 <= Plast) issue(K + HH + 1);
       {
         bool got = true;
         const int wlast = flat ? K : K + HH;
@@ -289,6 +288,11 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         if (tid == 0)
           for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= wlast; ++pl) pending &= ~(1u << pmod(pl, C::NSLOT));
       }
+      // Prefetch plane K+HH+1 into the slot of plane K-1.  Issued after the
+      // barrier above, which every thread reaches only after its last read of
+      // plane K-1 (the previous step's output phase), so the steps need no
+      // barrier at their end.
+      if (tid == 0 && K > Kfirst && K + HH + 1 <= Plast) issue(K + HH + 1);
       const int sK = pmod(K, C::NSLOT), sK1 = pmod(K + 1, C::NSLOT), sK2 = pmod(K + 2, C::NSLOT);
       // ring bases of planes K, K+1, K+2 (uniform, once per step)
       const Real* uK = uring + sK * C::SLOT;
@@ -723,8 +727,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         }
         if (bad) atomicOr(p.status, bad);
       }
-      __syncthreads();
     }
+    __syncthreads();  // the next tile's first loads reuse every ring slot
   }
   if constexpr (STAGED) cp_async_wait_all();  // none left in flight at exit
   // On a timeout, wait (bounded) for every load this block may still have in flight.
