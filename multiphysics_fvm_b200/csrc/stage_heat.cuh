@@ -116,7 +116,6 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
     };
     if (tid == 0) issue(Pfirst);
     for (int K = Kfirst; K <= Zl; ++K) {
-      if (tid == 0 && K + HH + 1 <= Plast) issue(K + HH + 1);
       {
         const int s = pmod(K + HH, C::NSLOT);
         const bool got = mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 2000000000ull);
@@ -128,6 +127,10 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         phase_bits ^= 1u << s;
         pending &= ~(1u << s);
       }
+      // Prefetch plane K+HH+1 into the slot of plane K-1.  Issued after the
+      // barrier above, which every thread reaches only after its last read of
+      // the previous step, so the steps need no barrier at their end.
+      if (tid == 0 && K + HH + 1 <= Plast) issue(K + HH + 1);
       // U0 and acc of this plane's output cell, loaded now so that the rest
       // of the step hides their latency
       Real eu0 = Real(0), eacc = Real(0);
@@ -227,7 +230,6 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
           if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
           if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
         }
-        __syncthreads();
         continue;
       }
       // x1 faces of plane K
@@ -294,8 +296,8 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
         if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
       }
-      __syncthreads();
     }
+    __syncthreads();  // the next tile's first loads reuse every ring slot
   }
   if (!ok && tid == 0)
     for (int s = 0; s < C::NSLOT; ++s)

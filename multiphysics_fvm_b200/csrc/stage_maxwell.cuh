@@ -165,7 +165,6 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
     };
     if (tid == 0) issue(Pfirst);
     for (int K = Kfirst; K <= Zl; ++K) {
-      if (tid == 0 && K + HH + 1 <= Plast) issue(K + HH + 1);
       {
         const int s = pmod(K + HH, C::NSLOT);
         const bool got = mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 2000000000ull);
@@ -177,6 +176,10 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
         phase_bits ^= 1u << s;
         pending &= ~(1u << s);
       }
+      // Prefetch plane K+HH+1 into the slot of plane K-1.  Issued after the
+      // barrier above, which every thread reaches only after its last read of
+      // the previous step, so the steps need no barrier at their end.
+      if (tid == 0 && K + HH + 1 <= Plast) issue(K + HH + 1);
       // U0 and acc of this plane's output cells, fetched now so that the
       // step hides their latency: copied into this thread's shared-memory
       // slots (STAGED), or lane 0 of each row asks L2 for them
@@ -449,8 +452,8 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
         }
         if (bad) atomicOr(p.status, bad);
       }
-      __syncthreads();
     }
+    __syncthreads();  // the next tile's first loads reuse every ring slot
   }
   if constexpr (STAGED) cp_async_wait_all();  // none left in flight at exit
   if (!ok && tid == 0)
