@@ -277,6 +277,13 @@ __global__ void __launch_bounds__(128, ConvCfg<CIN, COUT>::MINB) conv3_kernel(co
                              __uint_as_float(v[4 * q + 3]) + bias[4 * q + 3]);
     } else {
       uint4* out = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(a.y) + pos * COUT);
+      // every mask load before the first store (the stores may alias the mask
+      // as far as the compiler knows: one memory round trip per chunk otherwise)
+      uint4 mks[EPI == EPI_MASK_BF16 ? COUT / 8 : 1];
+      if constexpr (EPI == EPI_MASK_BF16) {
+#pragma unroll
+        for (int q = 0; q < COUT / 8; ++q) mks[q] = ldg16(a.mask + pos * COUT + 8 * q);
+      }
 #pragma unroll
       for (int q = 0; q < COUT / 8; ++q) {
         float f[8];
@@ -286,7 +293,7 @@ __global__ void __launch_bounds__(128, ConvCfg<CIN, COUT>::MINB) conv3_kernel(co
 #pragma unroll
           for (int e = 0; e < 8; ++e) f[e] = fmaxf(f[e] + bias[8 * q + e], 0.f);
         } else {
-          const uint4 mk = ldg16(a.mask + pos * COUT + 8 * q);
+          const uint4 mk = mks[q];
           const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
