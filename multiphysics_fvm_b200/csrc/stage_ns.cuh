@@ -270,13 +270,18 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
     if (tid == 0)
       for (int pl = Pfirst; pl <= Kfirst + HH + 1 && pl <= Plast; ++pl) issue(pl);
 
-    for (int K = Kfirst; K <= Zl; ++K) {
+    // Ring slots of plane K+d, d >= 0 small: bu = K mod NSLOT and b3 = K mod 3
+    // are carried from step to step, so each slot is a compare and subtract.
+    for (int K = Kfirst, bu = pmod(Kfirst, C::NSLOT), b3 = pmod(Kfirst, 3); K <= Zl;
+         ++K, bu = (bu + 1 == C::NSLOT ? 0 : bu + 1), b3 = (b3 == 2 ? 0 : b3 + 1)) {
+      auto su = [&](int d) { const int t = bu + d; return t >= C::NSLOT ? t - C::NSLOT : t; };  // d < NSLOT
+      auto s3 = [&](int d) { const int t = b3 + d; return t >= 3 ? t - 3 : t; };                // d <= 3
       // ---------------------------------------------------------- A ----
       {
         bool got = true;
         const int wlast = flat ? K : K + HH;
         for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= wlast; ++pl) {
-          const int s = pmod(pl, C::NSLOT);
+          const int s = su(pl - K);
           got = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 2000000000ull);
           phase_bits ^= (1u << s);
         }
@@ -286,24 +291,24 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
           break;
         }
         if (tid == 0)
-          for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= wlast; ++pl) pending &= ~(1u << pmod(pl, C::NSLOT));
+          for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= wlast; ++pl) pending &= ~(1u << su(pl - K));
       }
       // Prefetch plane K+HH+1 into the slot of plane K-1.  Issued after the
       // barrier above, which every thread reaches only after its last read of
       // plane K-1 (the previous step's output phase), so the steps need no
       // barrier at their end.
       if (tid == 0 && K > Kfirst && K + HH + 1 <= Plast) issue(K + HH + 1);
-      const int sK = pmod(K, C::NSLOT), sK1 = pmod(K + 1, C::NSLOT), sK2 = pmod(K + 2, C::NSLOT);
+      const int sK = su(0), sK1 = su(1), sK2 = su(2);
       // ring bases of planes K, K+1, K+2 (uniform, once per step)
       const Real* uK = uring + sK * C::SLOT;
       const Real* uK1 = uring + sK1 * C::SLOT;
       const Real* uK2 = uring + sK2 * C::SLOT;
-      const Real* pK = pring + pmod(K, 3) * PL2;
-      const Real* pK1 = pring + pmod(K + 1, 3) * PL2;
-      const Real* pK2 = pring + pmod(K + 2, 3) * PL2;
-      const Real* tK = tring + pmod(K, 3) * 6 * PL2;
-      const Real* tK1 = tring + pmod(K + 1, 3) * 6 * PL2;
-      const Real* tK2 = tring + pmod(K + 2, 3) * 6 * PL2;
+      const Real* pK = pring + s3(0) * PL2;
+      const Real* pK1 = pring + s3(1) * PL2;
+      const Real* pK2 = pring + s3(2) * PL2;
+      const Real* tK = tring + s3(0) * 6 * PL2;
+      const Real* tK1 = tring + s3(1) * 6 * PL2;
+      const Real* tK2 = tring + s3(2) * 6 * PL2;
       // U0 and acc of this plane's output cells, fetched here so that the
       // whole step hides their latency: into registers (EARLY), into this
       // thread's shared-memory slots (STAGED), or else lane 0 of each output
@@ -336,8 +341,8 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       // v on the newest plane(s), tile + 3 (viscous only)
       if constexpr (VISC) {
         for (int pl = (K == Kfirst ? Pfirst : K + 3); pl <= K + 3; ++pl) {
-          const Real* ub = uring + pmod(pl, C::NSLOT) * C::SLOT;
-          Real* vb = vring + pmod(pl, 3) * 3 * PL;
+          const Real* ub = uring + su(pl - K) * C::SLOT;  // pl - K in 1..3
+          Real* vb = vring + s3(pl - K) * 3 * PL;
           for (int it = tid; it < C::ROWS * (TX + 6); it += NT) {
             const int r = it / (TX + 6), c = 1 + it % (TX + 6);
             const int o = r * W + c;
@@ -358,7 +363,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       // ---------------------------------------------------------- C ----
       // P on plane K+2, tile + 2 (navier_stokes.py:94-100); with viscosity it
       // is formed inside the stress loop below (same cells)
-      Real* const pw = pring + pmod(flat ? K : K + 2, 3) * PL2;
+      Real* const pw = pring + s3(flat ? 0 : 2) * PL2;
       const Real* const usrc = flat ? uK : uK2;
       auto pressure_at = [&](int it) {
         const int r2 = it / W2, c2 = it % W2;
@@ -386,10 +391,10 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         const int pl = K + 2;
         const int k = pl - 1;  // interior plane index
         const bool zghost = (k < 0 || k >= nz);
-        const Real* vm = vring + pmod(pl - 1, 3) * 3 * PL;  // v of planes K+1, K+2, K+3
-        const Real* v0p = vring + pmod(pl, 3) * 3 * PL;
-        const Real* vp = vring + pmod(pl + 1, 3) * 3 * PL;
-        Real* tw = tring + pmod(pl, 3) * 6 * PL2;
+        const Real* vm = vring + s3(1) * 3 * PL;  // v of planes K+1, K+2, K+3
+        const Real* v0p = vring + s3(2) * 3 * PL;
+        const Real* vp = vring + s3(3) * 3 * PL;
+        Real* tw = tring + s3(2) * 6 * PL2;
         for (int it = tid; it < C::PL2; it += NT) {
           pressure_at(it);
           const int r2 = it / W2, c2 = it % W2;
@@ -499,9 +504,9 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         const int hh = tid - TX * TY, row = hh & 31;
         if (!is_out && row < TY && Kh >= Z0 && Kh <= Zl) {
           constexpr int ti[3] = {0, 3, 4};  // tau row 1 = (t11, t12, t13)
-          const Real* uh = uring + pmod(Kh, C::NSLOT) * C::SLOT;
-          const Real* ph = pring + pmod(Kh, 3) * PL2;
-          const Real* th = tring + pmod(Kh, 3) * 6 * PL2;
+          const Real* uh = uring + su(Kh - K) * C::SLOT;
+          const Real* ph = pring + s3(Kh - K) * PL2;
+          const Real* th = tring + s3(Kh - K) * 6 * PL2;
           const int kh = Kh - 1, j = y0 + row, par = Kh & 1;
           if (hh < 32) {
             const int i = x0 - 1;
