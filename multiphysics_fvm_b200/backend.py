@@ -375,10 +375,8 @@ def cached_simulation(physics: str, grid: dict, params: dict, space_schemes: dic
         raise ValueError("grid dict lacks 'coordinate_system': build it with multiphysics_fvm_b200.grid.geometry.build_grid")
     prec = precision or grid.get("precision", "fp64")
     if bcs is None:  # residual-only use: any valid BC set
-        p = ("periodic",)
         from .grid import boundary_conditions as bcm
         bcs = {v: {s: bcm.periodic for s in SIDES} for v in VARIABLES[physics]}
-        del p
     key = (physics, cs, _key(grid["config"]), _key(params), _key(space_schemes), _key(bcs), _key(integrator), prec)
     return CACHE.get(key, lambda: Simulation(physics, cs, grid["config"], params, space_schemes, bcs,
                                              integrator, precision=prec))

@@ -18,7 +18,6 @@ from __future__ import annotations
 import inspect
 import math
 
-import numpy as np
 
 from . import backend
 from . import io
