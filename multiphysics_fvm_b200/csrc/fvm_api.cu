@@ -386,6 +386,19 @@ struct Prof {
   cudaEvent_t a = nullptr, b = nullptr;
   double stage_ms = 0.0, other_ms = 0.0;
   int stage_launches = 0;
+  ~Prof() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+// Two CUDA events, destroyed on every return path.
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
 };
 
 // Enqueue one time step on the handle's stream: [dt reduction], clock, then
@@ -776,18 +789,16 @@ int fvm_time_steps(fvm_handle* h, int n_steps, int dt_mode, double* ms) {
   if (dt_mode != 0 && dt_mode != 1) return fail(FVM_E_INVALID, "dt_mode must be 0 (CFL) or 1 (fixed)");
   int rc = ensure_graph(h, dt_mode);
   if (rc) return rc;
-  cudaEvent_t a, b;
-  FVM_CK(cudaEventCreate(&a));
-  FVM_CK(cudaEventCreate(&b));
+  EventPair ev;
+  FVM_CK(cudaEventCreate(&ev.a));
+  FVM_CK(cudaEventCreate(&ev.b));
   FVM_CK(cudaStreamSynchronize(h->stream));
-  FVM_CK(cudaEventRecord(a, h->stream));
+  FVM_CK(cudaEventRecord(ev.a, h->stream));
   for (int s = 0; s < n_steps; ++s) FVM_CK(cudaGraphLaunch(h->graph[dt_mode], h->stream));
-  FVM_CK(cudaEventRecord(b, h->stream));
-  FVM_CK(cudaEventSynchronize(b));
+  FVM_CK(cudaEventRecord(ev.b, h->stream));
+  FVM_CK(cudaEventSynchronize(ev.b));
   float t = 0.f;
-  FVM_CK(cudaEventElapsedTime(&t, a, b));
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  FVM_CK(cudaEventElapsedTime(&t, ev.a, ev.b));
   *ms = t;
   return FVM_OK;
 }
@@ -841,8 +852,6 @@ int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_ker
   FVM_CK(cudaEventCreate(&pf.b));
   int rc = FVM_OK;
   for (int s = 0; s < n_steps && !rc; ++s) rc = enqueue_step(h, dt_mode, &pf);
-  cudaEventDestroy(pf.a);
-  cudaEventDestroy(pf.b);
   if (rc) return rc;
   FVM_CK(cudaStreamSynchronize(h->stream));
   if (stage_kernel_ms) *stage_kernel_ms = pf.stage_ms;
@@ -1240,17 +1249,15 @@ int fvm_batch_time_steps(fvm_batch* b, int n_steps, int dt_mode, double* ms) {
   if (dt_mode != 0 && dt_mode != 1) return fail(FVM_E_INVALID, "dt_mode must be 0 (CFL) or 1 (fixed)");
   int rc = batch_graph(b, dt_mode);
   if (rc) return rc;
-  cudaEvent_t e0, e1;
-  FVM_CK(cudaEventCreate(&e0));
-  FVM_CK(cudaEventCreate(&e1));
-  FVM_CK(cudaEventRecord(e0, b->stream));
+  EventPair ev;
+  FVM_CK(cudaEventCreate(&ev.a));
+  FVM_CK(cudaEventCreate(&ev.b));
+  FVM_CK(cudaEventRecord(ev.a, b->stream));
   for (int s = 0; s < n_steps; ++s) FVM_CK(cudaGraphLaunch(b->graph[dt_mode], b->stream));
-  FVM_CK(cudaEventRecord(e1, b->stream));
-  FVM_CK(cudaEventSynchronize(e1));
+  FVM_CK(cudaEventRecord(ev.b, b->stream));
+  FVM_CK(cudaEventSynchronize(ev.b));
   float t = 0.f;
-  FVM_CK(cudaEventElapsedTime(&t, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  FVM_CK(cudaEventElapsedTime(&t, ev.a, ev.b));
   *ms = t;
   return FVM_OK;
 }
