@@ -235,12 +235,14 @@ FixArgs fix_args(fvm_closure* c, const float* uin, float* uout, const Layout& la
 
 // The correction of one stage: clip-only, or the two FCT passes.
 cudaError_t launch_fix(fvm_closure* c, const FixArgs& a, cudaStream_t s) {
+  // one block of 128 threads per x1 row (for_each_cell)
+  const int rows = a.lay.ny * a.lay.nz;
   if (c->fct) {
-    fct_ratio_kernel<<<4 * c->nsm, 256, 0, s>>>(a);
+    fct_ratio_kernel<<<rows, 128, 0, s>>>(a);
     CL_RET(cudaGetLastError());
-    fct_apply_kernel<<<4 * c->nsm, 256, 0, s>>>(a);
+    fct_apply_kernel<<<rows, 128, 0, s>>>(a);
   } else {
-    closure_fix_kernel<<<4 * c->nsm, 256, 0, s>>>(a);
+    closure_fix_kernel<<<rows, 128, 0, s>>>(a);
   }
   return cudaGetLastError();
 }

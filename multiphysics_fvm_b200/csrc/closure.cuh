@@ -815,7 +815,7 @@ __device__ __forceinline__ float wave_speed(const float* u, int ax, float gamma)
 // on its -x_ax face (the +face of the neighbour below), and the dense
 // indices of the six neighbours (nb[ax][0] = -e_ax, nb[ax][1] = +e_ax).
 __device__ __forceinline__ void face_corrections(const FixArgs& a, const int c[3], long long p, float Fp[3][5],
-                                                 float Fm[3][5], long long nb[3][2]) {
+                                                 float Fm[3][5], long long nb[3][2], int nc[3][2][3] = nullptr) {
   const Layout& L = a.lay;
   const int dims[3] = {L.nx, L.ny, L.nz};
   float u0[5];
@@ -823,8 +823,12 @@ __device__ __forceinline__ void face_corrections(const FixArgs& a, const int c[3
 #pragma unroll
   for (int ax = 0; ax < 3; ++ax) {
     int cp[3] = {c[0], c[1], c[2]}, cm[3] = {c[0], c[1], c[2]};
-    cp[ax] = (c[ax] + 1) % dims[ax];
-    cm[ax] = (c[ax] + dims[ax] - 1) % dims[ax];
+    cp[ax] = c[ax] + 1 == dims[ax] ? 0 : c[ax] + 1;  // periodic neighbours
+    cm[ax] = c[ax] == 0 ? dims[ax] - 1 : c[ax] - 1;
+    if (nc) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) { nc[ax][0][d] = cm[d]; nc[ax][1][d] = cp[d]; }
+    }
     float up[5], um[5];
     load_cell(a, cp[0], cp[1], cp[2], up);
     load_cell(a, cm[0], cm[1], cm[2], um);
@@ -856,13 +860,27 @@ __device__ __forceinline__ void gated_store(const FixArgs& a, const int c[3], co
   }
 }
 
-__global__ void __launch_bounds__(256) closure_fix_kernel(const FixArgs a) {
+// Interior cells of the correction kernels: one x1 row per block iteration,
+// threads along the row, so (i, j, k) and the dense index p = row * nx + i
+// need no 64-bit division.
+template <class Body>
+__device__ __forceinline__ void for_each_cell(const Layout& L, Body body) {
+  const int rows = L.ny * L.nz;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int j = row % L.ny, k = row / L.ny;
+    const long long p0 = (long long)row * L.nx;
+    for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
+      const int c[3] = {i, j, k};
+      body(c, p0 + i);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) closure_fix_kernel(const FixArgs a) {
   if (a.clk && !a.clk->active) return;
   const float cdt = a.coef * (a.clk ? (float)a.clk->dt : a.dt_host);
   const Layout& L = a.lay;
-  const long long n = (long long)L.nx * L.ny * L.nz;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    const int c[3] = {(int)(p % L.nx), (int)((p / L.nx) % L.ny), (int)(p / ((long long)L.nx * L.ny))};
+  for_each_cell(L, [&](const int c[3], long long p) {
     float Fp[3][5], Fm[3][5];
     long long nb[3][2];
     face_corrections(a, c, p, Fp, Fm, nb);
@@ -875,7 +893,7 @@ __global__ void __launch_bounds__(256) closure_fix_kernel(const FixArgs a) {
       un[q] = a.uout[L.idx(q, c[2] + 1, c[1] + 1, c[0] + 1)] + cdt * r;
     }
     gated_store(a, c, un);
-  }
+  });
 }
 
 // Flux-corrected transport (Zalesak 1979) bound on the corrections: the
@@ -884,16 +902,16 @@ __global__ void __launch_bounds__(256) closure_fix_kernel(const FixArgs a) {
 // corrections create no new extrema.  Pass 1: per cell and variable the
 // fractions R+ (of the summed inflows) and R- (of the summed outflows) that
 // fit inside those bounds, ratio[q][p] and ratio[5+q][p].
-__global__ void __launch_bounds__(256) fct_ratio_kernel(const FixArgs a) {
+__global__ void __launch_bounds__(128) fct_ratio_kernel(const FixArgs a) {
   if (a.clk && !a.clk->active) return;
   const float cdt = a.coef * (a.clk ? (float)a.clk->dt : a.dt_host);
   const Layout& L = a.lay;
   const long long n = (long long)L.nx * L.ny * L.nz;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    const int c[3] = {(int)(p % L.nx), (int)((p / L.nx) % L.ny), (int)(p / ((long long)L.nx * L.ny))};
+  for_each_cell(L, [&](const int c[3], long long p) {
     float Fp[3][5], Fm[3][5];
     long long nb[3][2];
-    face_corrections(a, c, p, Fp, Fm, nb);
+    int nc[3][2][3];
+    face_corrections(a, c, p, Fp, Fm, nb, nc);
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
       const float ul = a.uout[L.idx(q, c[2] + 1, c[1] + 1, c[0] + 1)];
@@ -906,9 +924,8 @@ __global__ void __launch_bounds__(256) fct_ratio_kernel(const FixArgs a) {
         pout += fmaxf(-tp, 0.f) + fmaxf(-tm, 0.f);
 #pragma unroll
         for (int sd = 0; sd < 2; ++sd) {
-          const long long m = nb[ax][sd];
-          const int mi = (int)(m % L.nx), mj = (int)((m / L.nx) % L.ny), mk = (int)(m / ((long long)L.nx * L.ny));
-          const float un = a.uout[L.idx(q, mk + 1, mj + 1, mi + 1)];
+          const int* m = nc[ax][sd];
+          const float un = a.uout[L.idx(q, m[2] + 1, m[1] + 1, m[0] + 1)];
           hi = fmaxf(hi, un);
           lo = fminf(lo, un);
         }
@@ -916,19 +933,18 @@ __global__ void __launch_bounds__(256) fct_ratio_kernel(const FixArgs a) {
       a.ratio[(long long)q * n + p] = pin > 0.f ? fminf(1.f, (hi - ul) / pin) : 1.f;
       a.ratio[(long long)(5 + q) * n + p] = pout > 0.f ? fminf(1.f, (ul - lo) / pout) : 1.f;
     }
-  }
+  });
 }
 
 // Pass 2: each face transfer T (from the lower to the upper cell) is scaled
 // by C = min(R+ of the receiving cell, R- of the giving cell), the same factor
 // seen from both cells, so the limited correction stays conservative.
-__global__ void __launch_bounds__(256) fct_apply_kernel(const FixArgs a) {
+__global__ void __launch_bounds__(128) fct_apply_kernel(const FixArgs a) {
   if (a.clk && !a.clk->active) return;
   const float cdt = a.coef * (a.clk ? (float)a.clk->dt : a.dt_host);
   const Layout& L = a.lay;
   const long long n = (long long)L.nx * L.ny * L.nz;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-    const int c[3] = {(int)(p % L.nx), (int)((p / L.nx) % L.ny), (int)(p / ((long long)L.nx * L.ny))};
+  for_each_cell(L, [&](const int c[3], long long p) {
     float Fp[3][5], Fm[3][5];
     long long nb[3][2];
     face_corrections(a, c, p, Fp, Fm, nb);
@@ -953,7 +969,7 @@ __global__ void __launch_bounds__(256) fct_apply_kernel(const FixArgs a) {
       un[q] = a.uout[L.idx(q, c[2] + 1, c[1] + 1, c[0] + 1)] + d;
     }
     gated_store(a, c, un);
-  }
+  });
 }
 
 }  // namespace closure
