@@ -129,7 +129,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline_sample(n=48, steps=2):
+CPU_N, CPU_STEPS = 96, 3  # about 10 s of one core: large enough that the arrays leave the caches
+
+
+def cpu_baseline_sample(n=CPU_N, steps=CPU_STEPS):
     """The CPU oracle on a bounded sample of the workload, one core."""
     from oracle import fvm_oracle as O
     s, U = make_state(n)
@@ -289,7 +292,8 @@ def run_ours(args):
                     "h2d_bytes_per_step": int(U.nbytes), "d2h_bytes_per_step": int(U.nbytes),
                     "how": "fvm_upload(pinned float64 state) + fvm_step(1) + fvm_download per step, wall clock"},
             "cpu_baseline": {"value": cpu_v, "unit": "cell-updates/s", "cores": 1, "kind": "port",
-                             "sample": f"CPU oracle, 48^3 RT cells, 2 rk3 steps ({cpu_el:.1f} s), NumPy float64"},
+                             "sample": f"CPU oracle, {CPU_N}^3 RT cells, {CPU_STEPS} rk3 steps ({cpu_el:.1f} s), "
+                                       "NumPy float64"},
             "clocks": clk.summary(),
             "closure": closure,
         }
