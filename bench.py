@@ -166,7 +166,7 @@ def run_reference(args):
         return 0
     import multiprocessing as mp
     cores = min(os.cpu_count() or 1, 64)
-    n = 32  # per-process sample: 32^3 cells of the same setup and schemes
+    n = 64  # per-process sample: 64^3 cells of the same setup and schemes (arrays larger than the caches)
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
         pool.map(_ref_worker, [(n, 1, 100 + i) for i in range(cores)])  # warm-up
