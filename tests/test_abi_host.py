@@ -61,6 +61,49 @@ def test_last_error_roundtrip():
     assert "coordinate system" in _lib.last_error()
 
 
+def _valid_desc():
+    from multiphysics_fvm_b200 import _lib
+    d = _lib.FvmDesc()
+    d.physics, d.precision, d.coords = 0, 0, 0
+    d.nx1 = d.nx2 = d.nx3 = 8
+    d.x1_max = d.x2_max = d.x3_max = 1.0
+    d.reconstructor, d.limiter, d.riemann, d.integrator = 1, 0, 1, 2
+    d.params[0] = 1.4
+    return d
+
+
+@pytest.mark.parametrize("field,value,message", [
+    ("precision", 7, "precision"),
+    ("nx2", 0, "grid sizes"),
+    ("nx1", 1 << 20, "grid too large"),
+    ("reconstructor", 2, "reconstructor"),
+    ("limiter", 3, "slope limiter"),
+    ("riemann", 2, "riemann"),
+    ("integrator", 4, "time integrator"),
+    ("tile_ty", 5, "tile_ty"),
+    ("bc", 4, "Unknown boundary condition"),
+    ("periodic_one_side", 1, "both sides"),
+])
+def test_descriptor_rules_rejected_before_any_cuda_call(field, value, message):
+    """fvm_create validates the descriptor first, so each rule is checked on
+    the CPU: the call returns FVM_E_INVALID (-1) and fvm_last_error names it."""
+    from multiphysics_fvm_b200 import _lib
+    lib = _lib.load()
+    d = _valid_desc()
+    if field == "nx1":
+        d.nx1 = d.nx2 = d.nx3 = value
+    elif field == "bc":
+        d.bc_kind[0][0] = value
+    elif field == "periodic_one_side":
+        d.bc_kind[2][2] = value  # neumann on the low x2 side, periodic on the high one
+    else:
+        setattr(d, field, value)
+    h = ctypes.c_void_p()
+    assert lib.fvm_create(ctypes.byref(d), ctypes.byref(h)) == -1
+    assert message in _lib.last_error()
+    assert not h.value
+
+
 def test_scheme_ids_accept_package_and_reference_callables():
     from multiphysics_fvm_b200 import backend, _lib as L
     from multiphysics_fvm_b200.numerics import riemann_solvers, slope_limiters, time_integrators
