@@ -9,6 +9,7 @@
 #include <limits>
 #include <mutex>
 #include <string>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/fvm.h"
@@ -1271,11 +1272,18 @@ int fvm_batch_time_steps(fvm_batch* b, int n_steps, int dt_mode, double* ms) {
 // of the coalesced 128-byte rows are fixed per kernel specialisation.
 namespace {
 
+// Depths: a fixed ladder plus ceil(nz / c) for every chunk count c (equal
+// chunks).  The persistent grid deals tiles round-robin, so a launch takes
+// ceil(tiles / resident blocks) tile times; some chunk count puts the tile
+// count just under a whole number of waves, and timing finds it.
 std::vector<int> zchunk_candidates(int nz) {
   std::vector<int> c;
   for (int z : {8, 16, 32, 48, 64, 96, 128, 192, 256})
     if (z < nz) c.push_back(z);
   c.push_back(nz);
+  for (int k = 2; k <= nz / 8; ++k) c.push_back((nz + k - 1) / k);
+  std::sort(c.begin(), c.end());
+  c.erase(std::unique(c.begin(), c.end()), c.end());
   return c;
 }
 
