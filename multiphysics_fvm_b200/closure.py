@@ -67,6 +67,7 @@ class Closure:
         self.npos = self.n[0] * self.n[1] * self.n[2]
         self.norm = None
         self.fct = False
+        self.meta = {}  # metadata of the loaded weights (selection beta, fct, ...)
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -138,7 +139,8 @@ class Closure:
         norm = json.loads(str(z["norm"]))
         if norm:
             self.set_norm(norm["gamma"], norm["in_mean"], norm["in_scale"], norm["out_scale"], norm["loss_weight"])
-        return json.loads(str(z["meta"])) if "meta" in z else {}
+        self.meta = json.loads(str(z["meta"])) if "meta" in z else {}
+        return self.meta
 
     # -- workspace access (tests) ----------------------------------------------
     def buffer(self, which: int) -> np.ndarray:
@@ -209,7 +211,15 @@ class Closure:
         return n.value
 
     # -- solver hook ---------------------------------------------------------------
-    def attach(self, sim, beta: float = 0.5):
+    # the clip factor used when neither the caller nor the weights' metadata gives one
+    DEFAULT_BETA = 0.05
+
+    def attach(self, sim, beta: float | None = None):
+        """Run the network in every step of ``sim``.  ``beta`` scales the face
+        clip; None takes the value the loaded weights were selected with
+        (their metadata), else DEFAULT_BETA."""
+        if beta is None:
+            beta = float(self.meta.get("beta", self.DEFAULT_BETA))
         L.check(self._lib.fvm_closure_attach(sim._h, self._h, float(beta)), "fvm_closure_attach")
         sim._closure = self  # keep the network alive while attached
 

@@ -56,8 +56,10 @@ def apply_ics(U: dict, params: dict, grid: dict, ics: dict) -> None:
 
 def _attach_closure(sim, spec):
     """Optional learned flux correction: ``setup["closure"] = {"weights": path
-    or closure.Closure, "beta": 0.5}`` (navier_stokes, fp32, cartesian,
-    periodic, rk3_ssp or euler_explicit)."""
+    or closure.Closure, "beta": 0.05, "fct": False}`` (navier_stokes, fp32,
+    cartesian, periodic, rk3_ssp or euler_explicit).  ``beta`` and ``fct`` are
+    optional: by default they are the values stored with the weights (the
+    ones the network was selected with)."""
     if not spec:
         return
     from . import closure
@@ -65,7 +67,11 @@ def _attach_closure(sim, spec):
     if not isinstance(net, closure.Closure):
         net = closure.Closure(sim.n)
         net.load(spec["weights"])
-    net.attach(sim, beta=float(spec.get("beta", 0.5)))
+    fct = spec.get("fct", net.meta.get("fct"))
+    if fct is not None:
+        net.set_limiter(bool(fct))
+    beta = spec.get("beta")
+    net.attach(sim, beta=None if beta is None else float(beta))
 
 
 def _advance(sim, k: int) -> int:

@@ -50,3 +50,30 @@ def test_trained_closure_beats_the_plain_coarse_run():
     assert closed["switched"] == 0
     for t, e_c, e_p in zip(row["t"], closed["err"], plain["err"]):
         assert e_c < 0.9 * e_p, f"t={t}: closure {e_c:.4f} vs plain {e_p:.4f}"
+
+
+def test_setup_closure_key_uses_the_weights_selection():
+    """solver.run(setup) with setup["closure"] = {"weights": path} and no beta
+    or fct attaches the network with the values stored with the weights: the
+    run ends bitwise equal to Simulation + Closure.attach(sim, beta=meta beta)."""
+    import math
+    from multiphysics_fvm_b200 import closure, solver
+    from multiphysics_fvm_b200.backend import Simulation
+    from multiphysics_fvm_b200.grid.geometry import build_grid
+    from multiphysics_fvm_b200.setups import kelvin_helmholtz_sharp as kh
+    meta = json.loads(str(np.load(WEIGHTS)["meta"]))
+    s = kh.get_setup(64, 64, 64, seed=7, n_steps=6, precision="fp32")
+    a = solver.run(dict(s, closure={"weights": WEIGHTS}), verbose=False)
+    U = s["physics"].allocate_u(s["grid_config"])
+    s["initial_conditions"]["initializer"](U, s["physical_parameters"], build_grid("cartesian", s["grid_config"]),
+                                           s["initial_conditions"]["parameters"])
+    b = Simulation.from_setup(s)
+    b.upload(U)
+    b.set_time(0.0, math.inf, 0.4)
+    net = closure.Closure(b.n)
+    net.load(WEIGHTS)
+    net.set_limiter(bool(meta.get("fct", False)))
+    net.attach(b, beta=float(meta["beta"]))
+    b.step(6)
+    assert a.status() == 0 and b.status() == 0
+    assert np.array_equal(a.download(), b.download())
