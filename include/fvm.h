@@ -195,7 +195,10 @@ int fvm_batch_autotune(fvm_batch* b, int* best_zchunk, double* best_ms_per_step)
  * array of nvars outputs.  nvars must be 1..8 (FVM_E_INVALID otherwise).  Work
  * is enqueued on `stream` (a cudaStream_t, 0 = legacy default stream) and not
  * waited for.  The first call on a device (with that device current) resolves
- * the array's device address; make it before any stream capture.  All calls
+ * the array's device address and keeps it for the process; that address
+ * belongs to the device's primary context, so it is not valid after
+ * cudaDeviceReset or in another driver-API context.  Make the first call
+ * before any stream capture.  All calls
  * share the one array: calls whose kernels can overlap on the GPU (other
  * streams, other host threads) race and must be serialised by the caller. */
 int fvm_totals_noalloc(const float* cells, const double* volumes, int nvars, long long ncells, double* totals,

@@ -74,3 +74,30 @@ def test_totals_noalloc_rejects_sizes_beyond_its_scratch():
     rc = lib.fvm_totals_noalloc(ctypes.c_void_p(cells.data_ptr()), ctypes.c_void_p(buf.data_ptr()), 9,
                                 ctypes.c_longlong(1), ctypes.c_void_p(buf.data_ptr()), None)
     assert rc == -1 and "nvars" in _lib.last_error()
+
+
+def test_totals_noalloc_full_scratch_against_numpy():
+    """80^3 cells (more than 1024 blocks of 256, so the grid-stride loop runs)
+    and nvars = 8 (every column of a scratch row), twice in a row, against a
+    float64 NumPy sum: relative <= 1e-12 of the sum of magnitudes."""
+    import torch
+    from multiphysics_fvm_b200 import _lib
+    lib = _lib.load()
+    n = 80 ** 3
+    out = torch.zeros(8, dtype=torch.float64, device="cuda")
+    for seed in (3, 4):
+        rng = np.random.default_rng(seed)
+        cells_h = rng.uniform(-1.0, 2.0, (8, n)).astype(np.float32)
+        vol_h = rng.uniform(0.5, 1.5, n) * 1e-6
+        cells = torch.tensor(cells_h, device="cuda")
+        vol = torch.tensor(vol_h, dtype=torch.float64, device="cuda")
+        out.fill_(123.0)
+        rc = lib.fvm_totals_noalloc(ctypes.c_void_p(cells.data_ptr()), ctypes.c_void_p(vol.data_ptr()), 8,
+                                    ctypes.c_longlong(n), ctypes.c_void_p(out.data_ptr()), None)
+        assert rc == 0, _lib.last_error()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        c64 = cells_h.astype(np.float64)
+        expect = np.sum(c64 * vol_h[None, :], axis=1)
+        scale = np.sum(np.abs(c64) * vol_h[None, :], axis=1)
+        assert np.all(np.abs(got - expect) <= 1e-12 * scale), (got, expect)
