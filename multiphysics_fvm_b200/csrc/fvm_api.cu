@@ -113,6 +113,9 @@ struct fvm_handle {
   double* stage_host = nullptr;  // pinned staging
   size_t stage_elems = 0;
   CUtensorMap tmap[3];
+  CUtensorMap smap{}, amap{};  // staged U0 / accumulator tiles of the float32 cartesian NS kernel
+  bool legacy = false;         // batch member: runs the batched (tile-list) kernels
+  unsigned long long wait_ns = 2000000000ull;  // limit of each wait for a TMA plane
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   double max_inv_l2 = 0.0, const_rate = 0.0;
   int zchunk = 64;
@@ -294,6 +297,7 @@ void fill_common(fvm_handle* h, const StageDef& sd, bool rhs_only, P& p) {
   p.coef.u0_is_input = sd.in == 0 ? 1 : 0;
   p.status = h->status;
   p.zchunk = h->zchunk;
+  p.wait_ns = h->wait_ns;
 }
 
 // x3 fluxes cancel exactly on a one-plane grid whose x3 ghosts copy the plane
@@ -841,6 +845,16 @@ int fvm_clear_status(fvm_handle* h) {
   if (!h) return fail(FVM_E_INVALID, "null handle");
   FVM_CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream));
   FVM_CK(cudaStreamSynchronize(h->stream));
+  return FVM_OK;
+}
+
+int fvm_set_wait_limit(fvm_handle* h, unsigned long long data_wait_ns) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  if (data_wait_ns == 0) return fail(FVM_E_INVALID, "fvm_set_wait_limit: the limit must be > 0 ns");
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  h->wait_ns = data_wait_ns;
+  for (auto& g : h->graph)  // the captured steps hold the old limit
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return FVM_OK;
 }
 

@@ -26,6 +26,7 @@ struct HeatParams {
   double rho_cp, k, q, inv_rho_cp;
   unsigned* status;
   int zchunk, ntx, nty, nzc;
+  unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
 };
 
 template <typename Real, int LIM, int TY>
@@ -118,7 +119,7 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
     for (int K = Kfirst; K <= Zl; ++K) {
       {
         const int s = pmod(K + HH, C::NSLOT);
-        const bool got = mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 2000000000ull);
+        const bool got = mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
         if (!__syncthreads_and(got)) {
           if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
           ok = false;

@@ -28,6 +28,7 @@ struct MaxwellParams {
   double mu, ep, sigma, rho_c, chi_b, chi_d, c;
   unsigned* status;
   int zchunk, ntx, nty, nzc;
+  unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
 };
 
 template <typename Real, int TY>
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
     for (int K = Kfirst; K <= Zl; ++K) {
       {
         const int s = pmod(K + HH, C::NSLOT);
-        const bool got = mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 2000000000ull);
+        const bool got = mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
         if (!__syncthreads_and(got)) {
           if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
           ok = false;

@@ -34,6 +34,7 @@ struct NsParams {
   unsigned* status;
   int zchunk, ntx, nty, nzc;
   int flat;  // nx3 == 1 with x3 ghosts equal to the plane: x3 fluxes cancel, no z-march
+  unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
 };
 
 // Tile sources: one grid (params + tensor map in kernel parameter space) or a
@@ -281,17 +282,22 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
         bool got = true;
         const int wlast = flat ? K : K + HH;
         for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= wlast; ++pl) {
+          // the phase bit flips (and thread 0 drops the slot from `pending`)
+          // only after a completed wait, so a drain after a timeout waits for
+          // the phase still outstanding
           const int s = su(pl - K);
-          got = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 2000000000ull);
-          phase_bits ^= (1u << s);
+          const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
+          if (g) {
+            phase_bits ^= (1u << s);
+            if (tid == 0) pending &= ~(1u << s);
+          }
+          got = g;
         }
         if (!__syncthreads_and(got)) {
           if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
           ok = false;
           break;
         }
-        if (tid == 0)
-          for (int pl = (K == Kfirst ? Pfirst : K + HH); pl <= wlast; ++pl) pending &= ~(1u << su(pl - K));
       }
       // Prefetch plane K+HH+1 into the slot of plane K-1.  Issued after the
       // barrier above, which every thread reaches only after its last read of
