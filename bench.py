@@ -304,17 +304,24 @@ def run_ours(args):
             if "traffic_source:" in line:
                 traffic_source = line.split("traffic_source:")[1].strip().rstrip("->").strip()
 
-    # end to end through the public API with host buffers: upload the float64
-    # ghosted state from pinned memory, one step, download it again
+    # end to end through the public API with host buffers: every step uploads
+    # the float64 ghosted state from pinned memory, advances one step and
+    # downloads the result; the pipelined calls overlap one step's upload with
+    # the previous step's download and compute
     host = torch.from_numpy(U).pin_memory().numpy()
     out = torch.empty(U.shape, dtype=torch.float64).pin_memory().numpy()
     e2e_steps = max(3, min(args.steps, 10))
+    sim.upload_async(host)  # first use makes the copy streams and staging buffer
+    sim.step_async(1)
+    sim.download_async(out)
+    sim.synchronize()
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        sim.upload(host)
-        sim.step(1)
-        sim.download(out)
+        sim.upload_async(host)
+        sim.step_async(1)
+        sim.download_async(out)
+    sim.synchronize()
     barrier()
     e2e_s = time.perf_counter() - t0
     e2e_s = reduce_max(dist, e2e_s)
@@ -344,7 +351,8 @@ def run_ours(args):
                                   "other_kernels": other_ms / (launches / len(STAGE_BYTES))},
             "e2e": {"value": e2e, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": int(U.nbytes), "d2h_bytes_per_step": int(U.nbytes),
-                    "how": "fvm_upload(pinned float64 state) + fvm_step(1) + fvm_download per step, wall clock"},
+                    "how": "fvm_upload_async(pinned float64 state) + fvm_step_async(1) + fvm_download_async per "
+                           "step, pipelined on two copy streams, wall clock to fvm_synchronize"},
             "cpu_baseline": {"value": cpu_v, "unit": "cell-updates/s", "cores": 1, "kind": "port",
                              "sample": f"CPU oracle, {CPU_N}^3 RT cells, {CPU_STEPS} rk3 steps ({cpu_el:.1f} s), "
                                        "NumPy float64"},

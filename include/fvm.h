@@ -103,6 +103,22 @@ int fvm_upload(fvm_handle* h, const double* host_state);
  * (src/io.py:14-63). */
 int fvm_download(fvm_handle* h, double* host_state);
 
+/* Pipelined transfers: the same copies as fvm_upload / fvm_download (the
+ * downloaded ghost edges and corners are averaged on the device, as
+ * src/solver.py:39-61), enqueued without waiting.  Uploads run on their own
+ * copy stream, downloads on another, so the upload of one step's input, the
+ * step (fvm_step_async) and the download of the previous result overlap.  Host
+ * buffers should be pinned (pageable memory makes the copy synchronous) and
+ * must stay valid and untouched until fvm_synchronize returns.  Replace the
+ * host-resident U of src/solver.py:64-85 and io.save_snapshot (src/io.py:14-63)
+ * when a caller streams states through the device. */
+int fvm_upload_async(fvm_handle* h, const double* host_state);
+int fvm_download_async(fvm_handle* h, double* host_state);
+/* fvm_step without waiting for the steps to finish (see fvm_step). */
+int fvm_step_async(fvm_handle* h, int n_steps, int dt_mode);
+/* Wait for everything enqueued on the handle (steps and pipelined copies). */
+int fvm_synchronize(fvm_handle* h);
+
 /* dt = CFL / max characteristic rate of the current state, reduced on the device
  * in float64.  Replaces physics.compute_dt (navier_stokes.py:512-585,
  * heat.py:305-351, maxwell.py:533-600). */

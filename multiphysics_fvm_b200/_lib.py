@@ -53,6 +53,10 @@ SIGNATURES = [
     ("fvm_info", C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
     ("fvm_upload", C.c_int, [_P, _DP]),
     ("fvm_download", C.c_int, [_P, _DP]),
+    ("fvm_upload_async", C.c_int, [_P, _DP]),
+    ("fvm_download_async", C.c_int, [_P, _DP]),
+    ("fvm_step_async", C.c_int, [_P, C.c_int, C.c_int]),
+    ("fvm_synchronize", C.c_int, [_P]),
     ("fvm_compute_dt", C.c_int, [_P, C.c_double, _DP]),
     ("fvm_residual", C.c_int, [_P, _DP]),
     ("fvm_step", C.c_int, [_P, C.c_int, C.c_int]),

@@ -199,6 +199,27 @@ class Simulation:
         L.check(self._lib.fvm_download(self._h, L.dptr(out)), "fvm_download")
         return out
 
+    def upload_async(self, U: np.ndarray):
+        """Enqueue the upload of a ghosted float64 state (NV, nx1+2, nx2+2,
+        nx3+2); ``U`` (pinned for a truly asynchronous copy) must stay alive and
+        unchanged until ``synchronize``."""
+        if U.shape != self._ghosted or U.dtype != np.float64 or not U.flags.c_contiguous:
+            raise ValueError(f"state must be C-contiguous float64 of shape {self._ghosted}")
+        L.check(self._lib.fvm_upload_async(self._h, L.dptr(U)), "fvm_upload_async")
+
+    def download_async(self, out: np.ndarray):
+        """Enqueue the download of the state into ``out`` (valid after ``synchronize``)."""
+        if out.shape != self._ghosted or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError(f"output must be C-contiguous float64 of shape {self._ghosted}")
+        L.check(self._lib.fvm_download_async(self._h, L.dptr(out)), "fvm_download_async")
+
+    def step_async(self, n_steps: int = 1):
+        """Enqueue n_steps CFL steps without waiting for them."""
+        L.check(self._lib.fvm_step_async(self._h, int(n_steps), 0), "fvm_step_async")
+
+    def synchronize(self):
+        L.check(self._lib.fvm_synchronize(self._h), "fvm_synchronize")
+
     def download_into(self, U: dict):
         arr = self.download()
         for q, k in enumerate(self.variables):

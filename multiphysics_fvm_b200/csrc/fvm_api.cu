@@ -112,6 +112,12 @@ struct fvm_handle {
   double* stage_dev = nullptr;   // reference-layout float64 staging on the device
   double* stage_host = nullptr;  // pinned staging
   size_t stage_elems = 0;
+  // pipelined host transfers (fvm_upload_async / fvm_download_async): a second
+  // device staging buffer for downloads, one stream per copy direction and the
+  // events that order them against the handle's stream
+  double* stage_out = nullptr;
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t ev_in_ready = nullptr, ev_in_free = nullptr, ev_out_ready = nullptr, ev_out_free = nullptr;
   CUtensorMap tmap[3];
   CUtensorMap smap{}, amap{};  // staged U0 / accumulator tiles of the float32 cartesian NS kernel
   bool legacy = false;         // batch member: runs the batched (tile-list) kernels
@@ -131,6 +137,18 @@ namespace {
 int default_tile_ty(const fvm_desc& d);
 int alt_tile_ty(const fvm_desc& d);
 int tile_halo(const fvm_desc& d);
+
+// float32 inviscid cartesian Navier-Stokes grids run the register-blocked
+// stage kernel (stage_ns_strip.cuh) and float32 piecewise-constant heat grids
+// stage_heat_pc.cuh; batch members keep the tile-list kernels.
+bool strip_desc(const fvm_desc& d) {
+  return d.precision == FVM_FP32 && d.physics == FVM_NAVIER_STOKES && d.coords == FVM_CARTESIAN && d.params[1] == 0.0;
+}
+bool strip_kernel(const fvm_handle* h) { return !h->legacy && strip_desc(h->d); }
+bool heat_pc_desc(const fvm_desc& d) {
+  return d.precision == FVM_FP32 && d.physics == FVM_HEAT && d.reconstructor == FVM_PIECEWISE_CONSTANT;
+}
+bool heat_pc_kernel(const fvm_handle* h) { return !h->legacy && heat_pc_desc(h->d); }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -164,11 +182,37 @@ int make_tmap(fvm_handle* h, int b, int rows) {
   return FVM_OK;
 }
 
-// Tensor maps of the three state buffers for the handle's tile rows.
+// 4D map of a staged tile (U0 or the k accumulator): 32 columns starting at
+// the tile's first interior column (16-byte aligned), `rows` rows, one plane,
+// all variables.
+int make_stage_tmap(fvm_handle* h, CUtensorMap* m, void* base, int rows) {
+  auto enc = get_encode();
+  if (!enc) return fail(FVM_E_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  const Layout& L = h->lay;
+  cuuint64_t dims[4] = {(cuuint64_t)(L.nx + 2 + L.padx), (cuuint64_t)(L.ny + 2), (cuuint64_t)(L.nz + 2),
+                        (cuuint64_t)h->nv};
+  cuuint64_t strides[3] = {(cuuint64_t)(L.pitch * h->esz), (cuuint64_t)(L.plane * h->esz),
+                           (cuuint64_t)(L.var_stride * h->esz)};
+  cuuint32_t box[4] = {32, (cuuint32_t)rows, 1, (cuuint32_t)h->nv};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(FVM_E_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return FVM_OK;
+}
+
+// Tensor maps of the three state buffers for the handle's tile rows (and the
+// staged-tile maps of the float32 cartesian NS kernel).
 int make_tmaps(fvm_handle* h) {
   const int rows = h->tile_ty + 2 * tile_halo(h->d);
   for (int b = 0; b < 3; ++b)
     if (int rc = make_tmap(h, b, rows)) return rc;
+  if (strip_kernel(h)) {
+    if (int rc = make_stage_tmap(h, &h->smap, h->U[0], h->tile_ty)) return rc;
+    if (h->acc)
+      if (int rc = make_stage_tmap(h, &h->amap, h->acc, h->tile_ty)) return rc;
+  }
   return FVM_OK;
 }
 
@@ -207,6 +251,8 @@ int kernel_limiter(const fvm_desc& d) {
 // one the float32 NS and heat kernels are also built with (equal if none).
 int default_tile_ty(const fvm_desc& d) {
   const bool f64 = d.precision == FVM_FP64, visc = d.physics == FVM_NAVIER_STOKES && d.params[1] != 0.0;
+  if (strip_desc(d)) return NS_STRIP_TY;
+  if (heat_pc_desc(d)) return HEAT_PC_TY;
   if (d.physics == FVM_HEAT) return HEAT_TY;
   if (d.physics == FVM_MAXWELL) return f64 ? maxwell_tile_ty<double>() : maxwell_tile_ty<float>();
   if (f64) return visc ? ns_tile_ty<double, true>() : ns_tile_ty<double, false>();
@@ -214,7 +260,9 @@ int default_tile_ty(const fvm_desc& d) {
 }
 int alt_tile_ty(const fvm_desc& d) {
   if (d.precision == FVM_FP64 || d.physics == FVM_MAXWELL) return default_tile_ty(d);
+  if (heat_pc_desc(d)) return HEAT_PC_TY_ALT;
   if (d.physics == FVM_HEAT) return HEAT_TY_ALT;
+  if (strip_desc(d)) return NS_STRIP_TY_ALT;
   return d.params[1] != 0.0 ? ns_tile_ty_alt<float, true>() : ns_tile_ty_alt<float, false>();
 }
 // Halo rows staged on each side of a tile (TMA box height = rows + 2*halo).
@@ -338,13 +386,24 @@ HeatParams<Real> make_heat_params(fvm_handle* h, const StageDef& sd, bool rhs_on
   return p;
 }
 
+// The float32 stage combination reads U0 from memory (fvm_common.cuh needs_u0).
+bool needs_u0_host(const StageDef& sd) {
+  return sd.mode >= MODE_AXPY && sd.mode != MODE_FINAL && sd.in != 0;
+}
+
 template <typename Real>
 cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool prepare_only = false) {
   const fvm_desc& d = h->d;
   const int nsm = prepare_only ? -1 : h->nsm;
-  if (d.physics == FVM_HEAT)
+  if (d.physics == FVM_HEAT) {
+    if constexpr (std::is_same<Real, float>::value) {
+      if (heat_pc_kernel(h))
+        return launch_heat_pc(d.coords, h->tmap[sd.in], make_heat_params<float>(h, sd, rhs_only), h->stream, nsm,
+                              h->tile_ty);
+    }
     return launch_heat<Real>(kernel_limiter(d), d.coords, h->tmap[sd.in], make_heat_params<Real>(h, sd, rhs_only),
                              h->stream, nsm, h->tile_ty);
+  }
   if (d.physics == FVM_MAXWELL) {
     MaxwellParams<Real> p{};
     fill_common<Real>(h, sd, rhs_only, p);
@@ -358,6 +417,17 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
     return launch_maxwell<Real>(kernel_limiter(d), d.riemann, d.coords, h->tmap[sd.in], p, h->stream, nsm);
   }
   const bool visc = d.params[1] != 0.0;
+  if constexpr (std::is_same<Real, float>::value) {
+    if (strip_kernel(h)) {
+      NsStripSource src;
+      src.tmap = h->tmap[sd.in];
+      src.u0map = h->smap;
+      src.accmap = h->amap;
+      src.p = make_ns_params<float>(h, sd, rhs_only);
+      const int nbuf = (needs_u0_host(sd) ? 1 : 0) + (sd.mode == MODE_FINAL || sd.accmode == ACC_ADD ? 1 : 0);
+      return launch_ns_strip(kernel_limiter(d), d.riemann, src, h->tile_ty, nbuf, h->stream, nsm);
+    }
+  }
   return launch_ns<Real>(kernel_limiter(d), d.riemann, d.coords, visc, h->tmap[sd.in],
                          make_ns_params<Real>(h, sd, rhs_only), h->stream, nsm, h->tile_ty);
 }
@@ -620,6 +690,13 @@ int fvm_destroy(fvm_handle* h) {
   if (h->totals_dev) cudaFree(h->totals_dev);
   if (h->stage_dev) cudaFree(h->stage_dev);
   if (h->stage_host) cudaFreeHost(h->stage_host);
+  if (h->s_in) cudaStreamSynchronize(h->s_in);
+  if (h->s_out) cudaStreamSynchronize(h->s_out);
+  if (h->stage_out) cudaFree(h->stage_out);
+  for (cudaEvent_t e : {h->ev_in_ready, h->ev_in_free, h->ev_out_ready, h->ev_out_free})
+    if (e) cudaEventDestroy(e);
+  if (h->s_in) cudaStreamDestroy(h->s_in);
+  if (h->s_out) cudaStreamDestroy(h->s_out);
   if (h->closure_nswitch) cudaFree(h->closure_nswitch);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -633,25 +710,26 @@ int fvm_info(const fvm_handle* h, int* nvars, long long* device_bytes) {
   return FVM_OK;
 }
 
-static int transpose(fvm_handle* h, bool to_device, int buf, bool interior) {
+static int transpose(fvm_handle* h, bool to_device, int buf, bool interior, double* stage = nullptr) {
   const fvm_desc& d = h->d;
+  if (!stage) stage = h->stage_dev;
   const int m1 = interior ? d.nx1 : d.nx1 + 2, m2 = interior ? d.nx2 : d.nx2 + 2, m3 = interior ? d.nx3 : d.nx3 + 2;
   const int off = interior ? 1 : 0;
   dim3 grid((m3 + 31) / 32, (m1 + 31) / 32, m2 * h->nv), block(32, 8);
   if (h->f64) {
     if (to_device)
-      transpose_kernel<double, true><<<grid, block, 0, h->stream>>>(h->stage_dev, nullptr, nullptr,
+      transpose_kernel<double, true><<<grid, block, 0, h->stream>>>(stage, nullptr, nullptr,
                                                                      static_cast<double*>(h->U[buf]), h->lay, m1, m2, m3, off);
     else
-      transpose_kernel<double, false><<<grid, block, 0, h->stream>>>(nullptr, h->stage_dev,
+      transpose_kernel<double, false><<<grid, block, 0, h->stream>>>(nullptr, stage,
                                                                       static_cast<const double*>(h->U[buf]), nullptr,
                                                                       h->lay, m1, m2, m3, off);
   } else {
     if (to_device)
-      transpose_kernel<float, true><<<grid, block, 0, h->stream>>>(h->stage_dev, nullptr, nullptr,
+      transpose_kernel<float, true><<<grid, block, 0, h->stream>>>(stage, nullptr, nullptr,
                                                                     static_cast<float*>(h->U[buf]), h->lay, m1, m2, m3, off);
     else
-      transpose_kernel<float, false><<<grid, block, 0, h->stream>>>(nullptr, h->stage_dev,
+      transpose_kernel<float, false><<<grid, block, 0, h->stream>>>(nullptr, stage,
                                                                      static_cast<const float*>(h->U[buf]), nullptr,
                                                                      h->lay, m1, m2, m3, off);
   }
@@ -708,6 +786,80 @@ int fvm_download(fvm_handle* h, double* host_state) {
   FVM_CK(cudaStreamSynchronize(h->stream));
   const size_t per = h->stage_elems / h->nv;
   for (int q = 0; q < h->nv; ++q) fill_edges_corners(host_state + q * per, h->d.nx1, h->d.nx2, h->d.nx3);
+  return FVM_OK;
+}
+
+namespace {
+// Streams, events and the second staging buffer of the pipelined transfers,
+// made on first use.
+int ensure_async(fvm_handle* h) {
+  if (h->s_in) return FVM_OK;
+  FVM_CK(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking));
+  FVM_CK(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&h->ev_in_ready, &h->ev_in_free, &h->ev_out_ready, &h->ev_out_free})
+    FVM_CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  const cudaError_t e = cudaMalloc(&h->stage_out, h->stage_elems * sizeof(double));
+  if (e != cudaSuccess) return fail(FVM_E_NOMEM, std::string("download staging: ") + cudaGetErrorString(e));
+  h->device_bytes += h->stage_elems * sizeof(double);
+  // nothing is in flight yet: both staging buffers start free
+  FVM_CK(cudaEventRecord(h->ev_in_free, h->stream));
+  FVM_CK(cudaEventRecord(h->ev_out_free, h->s_out));
+  return FVM_OK;
+}
+}  // namespace
+
+int fvm_upload_async(fvm_handle* h, const double* host_state) {
+  if (!h || !host_state) return fail(FVM_E_INVALID, "null argument");
+  int rc = ensure_async(h);
+  if (rc) return rc;
+  // copy stream: wait until the previous upload's transpose has read the
+  // staging buffer, then copy; the handle's stream transposes once it lands
+  FVM_CK(cudaStreamWaitEvent(h->s_in, h->ev_in_free, 0));
+  FVM_CK(cudaMemcpyAsync(h->stage_dev, host_state, h->stage_elems * sizeof(double), cudaMemcpyHostToDevice, h->s_in));
+  FVM_CK(cudaEventRecord(h->ev_in_ready, h->s_in));
+  FVM_CK(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
+  if ((rc = transpose(h, true, 0, false))) return rc;
+  FVM_CK(cudaEventRecord(h->ev_in_free, h->stream));
+  return FVM_OK;
+}
+
+int fvm_download_async(fvm_handle* h, double* host_state) {
+  if (!h || !host_state) return fail(FVM_E_INVALID, "null argument");
+  int rc = ensure_async(h);
+  if (rc) return rc;
+  FVM_CK(launch_bc(h, 0, false));
+  // the previous download's copy must have drained the staging buffer
+  FVM_CK(cudaStreamWaitEvent(h->stream, h->ev_out_free, 0));
+  if ((rc = transpose(h, false, 0, false, h->stage_out))) return rc;
+  const fvm_desc& d = h->d;
+  const int longest = std::max(d.nx1, std::max(d.nx2, d.nx3));
+  edges_kernel<<<dim3((longest + 255) / 256, 12 * h->nv), 256, 0, h->stream>>>(h->stage_out, d.nx1, d.nx2, d.nx3);
+  FVM_CK(cudaGetLastError());
+  corners_kernel<<<1, 64, 0, h->stream>>>(h->stage_out, d.nx1, d.nx2, d.nx3, h->nv);
+  FVM_CK(cudaGetLastError());
+  FVM_CK(cudaEventRecord(h->ev_out_ready, h->stream));
+  FVM_CK(cudaStreamWaitEvent(h->s_out, h->ev_out_ready, 0));
+  FVM_CK(cudaMemcpyAsync(host_state, h->stage_out, h->stage_elems * sizeof(double), cudaMemcpyDeviceToHost,
+                         h->s_out));
+  FVM_CK(cudaEventRecord(h->ev_out_free, h->s_out));
+  return FVM_OK;
+}
+
+int fvm_step_async(fvm_handle* h, int n_steps, int dt_mode) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  if (dt_mode != 0 && dt_mode != 1) return fail(FVM_E_INVALID, "dt_mode must be 0 (CFL) or 1 (fixed)");
+  if (n_steps <= 0) return FVM_OK;
+  int rc = ensure_graph(h, dt_mode);
+  if (rc) return rc;
+  for (int s = 0; s < n_steps; ++s) FVM_CK(cudaGraphLaunch(h->graph[dt_mode], h->stream));
+  return FVM_OK;
+}
+
+int fvm_synchronize(fvm_handle* h) {
+  if (!h) return fail(FVM_E_INVALID, "null handle");
+  FVM_CK(cudaStreamSynchronize(h->stream));
+  if (h->s_in) FVM_CK(cudaStreamSynchronize(h->s_in));
+  if (h->s_out) FVM_CK(cudaStreamSynchronize(h->s_out));
   return FVM_OK;
 }
 
@@ -1167,9 +1319,14 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     fvm_handle* h = nullptr;
     fvm_desc di = descs[i];
     di.tile_ty = 0;  // the batched kernels use each physics' default block shape
-    const int rc = fvm_create(&di, &h);
+    int rc = fvm_create(&di, &h);
     if (rc) return bail(rc);
     b->h.push_back(h);
+    if (strip_desc(di) || heat_pc_desc(di)) {  // the tile-list kernels' shape, not the single-grid kernel's
+      h->legacy = true;
+      h->tile_ty = strip_desc(di) ? ns_tile_ty<float, false>() : HEAT_TY;
+      if ((rc = make_tmaps(h))) return bail(rc);
+    }
   }
   // group by kernel specialisation
   for (int i = 0; i < n; ++i) {

@@ -80,6 +80,41 @@ __global__ void bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc
 // Reference layout (C order, last axis fastest) <-> device layout (x1 fastest).
 // src/dst reference arrays have dims (nv, m1, m2, m3) and map to ghosted device
 // indices g = m + off.  32x32 shared-memory tiles over (x1, x3) per (var, x2).
+// Ghost edges and corners of a reference-layout float64 state (NV, n1+2,
+// n2+2, n3+2) on the device, as src/solver.py:39-61: an edge is the mean of
+// the two adjacent ghost faces, a corner the mean of the three adjacent ghost
+// edges.  Edges read only face cells, so they are independent; corners run
+// after them.  blockIdx.y = variable * 12 + edge.
+__global__ void edges_kernel(double* f, int n1, int n2, int n3) {
+  const int N[3] = {n1 + 2, n2 + 2, n3 + 2};
+  const int q = blockIdx.y / 12, e = blockIdx.y % 12;
+  const int pair = e >> 2, ea = (e >> 1) & 1, eb = e & 1;
+  const int a = pair == 2 ? 1 : 0, b = pair == 0 ? 1 : 2, c = 3 - a - b;
+  double* g = f + (long long)q * N[0] * N[1] * N[2];
+  for (int t = 1 + blockIdx.x * blockDim.x + threadIdx.x; t <= N[c] - 2; t += gridDim.x * blockDim.x) {
+    int idx[3], pi[3], qi[3];
+    idx[a] = ea ? N[a] - 1 : 0;
+    idx[b] = eb ? N[b] - 1 : 0;
+    idx[c] = t;
+    for (int z = 0; z < 3; ++z) { pi[z] = idx[z]; qi[z] = idx[z]; }
+    pi[a] = ea ? N[a] - 2 : 1;
+    qi[b] = eb ? N[b] - 2 : 1;
+    auto at = [&](const int* x) -> double& { return g[((long long)x[0] * N[1] + x[1]) * N[2] + x[2]]; };
+    at(idx) = 0.5 * (at(pi) + at(qi));
+  }
+}
+__global__ void corners_kernel(double* f, int n1, int n2, int n3, int nv) {
+  const int N[3] = {n1 + 2, n2 + 2, n3 + 2};
+  const int id = threadIdx.x;
+  if (id >= 8 * nv) return;
+  const int q = id >> 3, ci = (id >> 2) & 1, cj = (id >> 1) & 1, ck = id & 1;
+  double* g = f + (long long)q * N[0] * N[1] * N[2];
+  auto at = [&](int i, int j, int k) -> double& { return g[((long long)i * N[1] + j) * N[2] + k]; };
+  const int i = ci ? N[0] - 1 : 0, j = cj ? N[1] - 1 : 0, k = ck ? N[2] - 1 : 0;
+  const int ii = ci ? N[0] - 2 : 1, jj = cj ? N[1] - 2 : 1, kk = ck ? N[2] - 2 : 1;
+  at(i, j, k) = (at(ii, j, k) + at(i, jj, k) + at(i, j, kk)) / 3.0;
+}
+
 template <typename Real, bool TO_DEVICE>
 __global__ void transpose_kernel(const double* __restrict__ hsrc, double* __restrict__ hdst,
                                  const Real* __restrict__ dsrc, Real* __restrict__ ddst, Layout L, int m1,

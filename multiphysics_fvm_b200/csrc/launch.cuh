@@ -3,7 +3,9 @@
 #pragma once
 #include <type_traits>
 #include "stage_ns.cuh"
+#include "stage_ns_strip.cuh"
 #include "stage_heat.cuh"
+#include "stage_heat_pc.cuh"
 #include "stage_maxwell.cuh"
 
 namespace fvm {
@@ -151,6 +153,44 @@ cudaError_t launch_ns(int lim, int riem, int coord, bool visc, const CUtensorMap
   return launch_ns_coord<Real, COORD_SPH>(lim, riem, visc, map, p, s, nsm, ty);
 }
 
+// ------------------------------------------------ float32 cartesian NS ----
+// Register-blocked stage kernel (stage_ns_strip.cuh) for float32 inviscid
+// cartesian grids: 4 rows per thread, TY = 16 (4 output warps) or 8 (2).
+constexpr int NS_STRIP_TY = 16, NS_STRIP_TY_ALT = 8;
+
+template <int LIM, int RIEM, int TY>
+cudaError_t launch_ns_strip_ty(const NsStripSource& src, int nbuf, cudaStream_t s, int nsm) {
+  constexpr int R = 4, NW = TY / R;
+  using C = NsStripCfg<R, NW>;
+  auto kern = ns_strip_kernel<LIM, RIEM, R, NW, TY == 16 ? 2 : 4>;
+  static int bps[3] = {0, 0, 0};
+  if (bps[0] == 0 || nsm < 0) {
+    // occupancy with 0, 1 and 2 staged tiles; the attribute ends at the largest
+    for (int nb = 0; nb < 3; ++nb) {
+      cudaError_t e = prepare_kernel(kern, C::NT, C::bytes(nb), &bps[nb]);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (nsm < 0) return cudaSuccess;
+  const long long ntiles = (long long)src.p.ntx * src.p.nty * src.p.nzc;
+  if (ntiles <= 0) return cudaSuccess;
+  const int grid = (int)(ntiles < (long long)bps[nbuf] * nsm ? ntiles : (long long)bps[nbuf] * nsm);
+  kern<<<grid, C::NT, C::bytes(nbuf), s>>>(src);
+  return cudaGetLastError();
+}
+
+template <int LIM, int RIEM>
+cudaError_t launch_ns_strip_lr(NsStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm) {
+  NsParams<float>& p = src.p;
+  p.ntx = (p.lay.nx + 31) / 32;
+  p.nty = (p.lay.ny + ty - 1) / ty;
+  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
+  if (ty == NS_STRIP_TY_ALT) return launch_ns_strip_ty<LIM, RIEM, NS_STRIP_TY_ALT>(src, nbuf, s, nsm);
+  return launch_ns_strip_ty<LIM, RIEM, NS_STRIP_TY>(src, nbuf, s, nsm);
+}
+
+cudaError_t launch_ns_strip(int lim, int riem, NsStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm);
+
 // ---------------------------------------------------------------- heat ----
 template <typename Real, int LIM, int COORD, class Src, int TY = HEAT_TY>
 cudaError_t launch_heat_src(const Src& src, long long ntiles, cudaStream_t s, int nsm) {
@@ -189,6 +229,30 @@ cudaError_t launch_heat_any(int lim, int coord, const Src& src, long long ntiles
 #undef FVM_HEAT_CASE
   return cudaErrorInvalidValue;
 }
+
+// Float32 piecewise-constant heat (stage_heat_pc.cuh): 4 rows per thread,
+// TY = 16 (4 warps) or 8 (2 warps).
+constexpr int HEAT_PC_TY = 16, HEAT_PC_TY_ALT = 8;
+
+template <int COORD, int TY>
+cudaError_t launch_heat_pc_ty(const CUtensorMap& map, const HeatParams<float>& p, cudaStream_t s, int nsm) {
+  constexpr int R = 4, NW = TY / R;
+  using C = HeatPcCfg<R, NW>;
+  auto kern = heat_pc_kernel<COORD, R, NW>;
+  static int bps = 0;
+  if (bps == 0 || nsm < 0) {
+    cudaError_t e = prepare_kernel(kern, C::NT, C::BYTES, &bps);
+    if (e != cudaSuccess) return e;
+  }
+  if (nsm < 0) return cudaSuccess;
+  const long long ntiles = (long long)p.ntx * p.nty * p.nzc;
+  if (ntiles <= 0) return cudaSuccess;
+  const int grid = (int)(ntiles < (long long)bps * nsm ? ntiles : (long long)bps * nsm);
+  kern<<<grid, C::NT, C::BYTES, s>>>(map, p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_heat_pc(int coord, const CUtensorMap& map, HeatParams<float> p, cudaStream_t s, int nsm, int ty);
 
 template <typename Real>
 cudaError_t launch_heat(int lim, int coord, const CUtensorMap& map, const HeatParams<Real>& p0, cudaStream_t s,
