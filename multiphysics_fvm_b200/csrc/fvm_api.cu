@@ -138,11 +138,12 @@ int default_tile_ty(const fvm_desc& d);
 int alt_tile_ty(const fvm_desc& d);
 int tile_halo(const fvm_desc& d);
 
-// float32 inviscid cartesian Navier-Stokes grids run the register-blocked
-// stage kernel (stage_ns_strip.cuh) and float32 piecewise-constant heat grids
-// stage_heat_pc.cuh; batch members keep the tile-list kernels.
+// float32 cartesian Navier-Stokes grids run the register-blocked stage
+// kernels (stage_ns_strip.cuh, stage_ns_strip_visc.cuh) and float32
+// piecewise-constant heat grids stage_heat_pc.cuh; batch members keep the
+// tile-list kernels.
 bool strip_desc(const fvm_desc& d) {
-  return d.precision == FVM_FP32 && d.physics == FVM_NAVIER_STOKES && d.coords == FVM_CARTESIAN && d.params[1] == 0.0;
+  return d.precision == FVM_FP32 && d.physics == FVM_NAVIER_STOKES && d.coords == FVM_CARTESIAN;
 }
 bool strip_kernel(const fvm_handle* h) { return !h->legacy && strip_desc(h->d); }
 bool heat_pc_desc(const fvm_desc& d) {
@@ -251,7 +252,7 @@ int kernel_limiter(const fvm_desc& d) {
 // one the float32 NS and heat kernels are also built with (equal if none).
 int default_tile_ty(const fvm_desc& d) {
   const bool f64 = d.precision == FVM_FP64, visc = d.physics == FVM_NAVIER_STOKES && d.params[1] != 0.0;
-  if (strip_desc(d)) return NS_STRIP_TY;
+  if (strip_desc(d)) return visc ? NS_STRIP_VISC_TY : NS_STRIP_TY;
   if (heat_pc_desc(d)) return HEAT_PC_TY;
   if (d.physics == FVM_HEAT) return HEAT_TY;
   if (d.physics == FVM_MAXWELL) return f64 ? maxwell_tile_ty<double>() : maxwell_tile_ty<float>();
@@ -262,7 +263,7 @@ int alt_tile_ty(const fvm_desc& d) {
   if (d.precision == FVM_FP64 || d.physics == FVM_MAXWELL) return default_tile_ty(d);
   if (heat_pc_desc(d)) return HEAT_PC_TY_ALT;
   if (d.physics == FVM_HEAT) return HEAT_TY_ALT;
-  if (strip_desc(d)) return NS_STRIP_TY_ALT;
+  if (strip_desc(d)) return d.params[1] != 0.0 ? NS_STRIP_VISC_TY_ALT : NS_STRIP_TY_ALT;
   return d.params[1] != 0.0 ? ns_tile_ty_alt<float, true>() : ns_tile_ty_alt<float, false>();
 }
 // Halo rows staged on each side of a tile (TMA box height = rows + 2*halo).
@@ -425,7 +426,8 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
       src.accmap = h->amap;
       src.p = make_ns_params<float>(h, sd, rhs_only);
       const int nbuf = (needs_u0_host(sd) ? 1 : 0) + (sd.mode == MODE_FINAL || sd.accmode == ACC_ADD ? 1 : 0);
-      return launch_ns_strip(kernel_limiter(d), d.riemann, src, h->tile_ty, nbuf, h->stream, nsm);
+      return visc ? launch_ns_strip_visc(kernel_limiter(d), d.riemann, src, h->tile_ty, nbuf, h->stream, nsm)
+                  : launch_ns_strip(kernel_limiter(d), d.riemann, src, h->tile_ty, nbuf, h->stream, nsm);
     }
   }
   return launch_ns<Real>(kernel_limiter(d), d.riemann, d.coords, visc, h->tmap[sd.in],
@@ -1324,7 +1326,8 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     b->h.push_back(h);
     if (strip_desc(di) || heat_pc_desc(di)) {  // the tile-list kernels' shape, not the single-grid kernel's
       h->legacy = true;
-      h->tile_ty = strip_desc(di) ? ns_tile_ty<float, false>() : HEAT_TY;
+      h->tile_ty = strip_desc(di) ? (di.params[1] != 0.0 ? ns_tile_ty<float, true>() : ns_tile_ty<float, false>())
+                                  : HEAT_TY;
       if ((rc = make_tmaps(h))) return bail(rc);
     }
   }

@@ -4,6 +4,7 @@
 #include <type_traits>
 #include "stage_ns.cuh"
 #include "stage_ns_strip.cuh"
+#include "stage_ns_strip_visc.cuh"
 #include "stage_heat.cuh"
 #include "stage_heat_pc.cuh"
 #include "stage_maxwell.cuh"
@@ -190,6 +191,42 @@ cudaError_t launch_ns_strip_lr(NsStripSource& src, int ty, int nbuf, cudaStream_
 }
 
 cudaError_t launch_ns_strip(int lim, int riem, NsStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm);
+
+// Viscous float32 cartesian grids (stage_ns_strip_visc.cuh): 2 rows per
+// thread, TY = 8 (4 output warps) or 4 (2).
+constexpr int NS_STRIP_VISC_TY = 8, NS_STRIP_VISC_TY_ALT = 4;
+
+template <int LIM, int RIEM, int TY>
+cudaError_t launch_ns_strip_visc_ty(const NsStripSource& src, int nbuf, cudaStream_t s, int nsm) {
+  constexpr int R = 2, NW = TY / R;
+  using C = NsStripViscCfg<R, NW>;
+  auto kern = ns_strip_visc_kernel<LIM, RIEM, R, NW, TY == 8 ? 2 : 3>;
+  static int bps[3] = {0, 0, 0};
+  if (bps[0] == 0 || nsm < 0) {
+    for (int nb = 0; nb < 3; ++nb) {
+      cudaError_t e = prepare_kernel(kern, C::NT, C::bytes(nb), &bps[nb]);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (nsm < 0) return cudaSuccess;
+  const long long ntiles = (long long)src.p.ntx * src.p.nty * src.p.nzc;
+  if (ntiles <= 0) return cudaSuccess;
+  const int grid = (int)(ntiles < (long long)bps[nbuf] * nsm ? ntiles : (long long)bps[nbuf] * nsm);
+  kern<<<grid, C::NT, C::bytes(nbuf), s>>>(src);
+  return cudaGetLastError();
+}
+
+template <int LIM, int RIEM>
+cudaError_t launch_ns_strip_visc_lr(NsStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm) {
+  NsParams<float>& p = src.p;
+  p.ntx = (p.lay.nx + 31) / 32;
+  p.nty = (p.lay.ny + ty - 1) / ty;
+  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
+  if (ty == NS_STRIP_VISC_TY_ALT) return launch_ns_strip_visc_ty<LIM, RIEM, NS_STRIP_VISC_TY_ALT>(src, nbuf, s, nsm);
+  return launch_ns_strip_visc_ty<LIM, RIEM, NS_STRIP_VISC_TY>(src, nbuf, s, nsm);
+}
+
+cudaError_t launch_ns_strip_visc(int lim, int riem, NsStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm);
 
 // ---------------------------------------------------------------- heat ----
 template <typename Real, int LIM, int COORD, class Src, int TY = HEAT_TY>

@@ -1,7 +1,8 @@
-"""The register-blocked float32 kernel for inviscid cartesian Navier-Stokes
-(stage_ns_strip.cuh) against the oracle, on grids that cut every kind of tile
-edge: several 32-column tiles with a partial last one, partial 16- and 8-row
-tiles, z-march chunks of a few planes (so chunk boundaries fall inside the
+"""The register-blocked float32 kernels for cartesian Navier-Stokes
+(stage_ns_strip.cuh inviscid, stage_ns_strip_visc.cuh with the Stokes stress)
+against the oracle, on grids that cut every kind of tile edge: several
+32-column tiles with a partial last one, partial row tiles of both block
+shapes, z-march chunks of a few planes (so chunk boundaries fall inside the
 grid), every limiter and both Riemann solvers, periodic and walled sides.
 
 Tolerances: single residual relative L-inf <= 2e-6 against the float64 oracle
@@ -22,6 +23,7 @@ pytestmark = pytest.mark.gpu
 N = (70, 40, 13)
 CFG = dict(x1_min=0.0, x1_max=1.0, x2_min=0.0, x2_max=0.7, x3_min=0.0, x3_max=0.4, nx1=N[0], nx2=N[1], nx3=N[2])
 PRM = {"heat_capacity_ratio": 1.4, "dynamic_viscosity": 0.0, "gravitational_acceleration": [0.2, -0.1, 0.3]}
+ALT = {0.0: 8, 0.02: 4}  # second block shape (tile rows) of each kernel
 LIMITERS = [("piecewise_constant", None), ("muscl", "minmod"), ("muscl", "monotonized_central"),
             ("muscl", "van_leer")]
 WALLS = [["periodic"] * 2 + ["neumann", ("dirichlet", 1.7), "neumann", "neumann"],
@@ -32,12 +34,12 @@ WALLS = [["periodic"] * 2 + ["neumann", ("dirichlet", 1.7), "neumann", "neumann"
 I3 = (slice(None),) + (slice(1, -1),) * 3
 
 
-def _sim(recon, lim, riem, kinds, tile_ty=0, zchunk=0, integrator="rk3_ssp", cfg=CFG):
+def _sim(recon, lim, riem, kinds, tile_ty=0, zchunk=0, integrator="rk3_ssp", cfg=CFG, prm=PRM):
     from multiphysics_fvm_b200.backend import Simulation
     from multiphysics_fvm_b200.numerics import reconstructors, riemann_solvers, slope_limiters, time_integrators
     sch = {"reconstructor": getattr(reconstructors, recon), "slope_limiter": getattr(slope_limiters, lim or "minmod"),
            "riemann_solver": getattr(riemann_solvers, riem)}
-    return Simulation("navier_stokes", "cartesian", cfg, PRM, sch, bcs_dict("navier_stokes", kinds),
+    return Simulation("navier_stokes", "cartesian", cfg, prm, sch, bcs_dict("navier_stokes", kinds),
                       getattr(time_integrators, integrator), precision="fp32", zchunk=zchunk, tile_ty=tile_ty)
 
 
@@ -45,33 +47,37 @@ def _osch(recon, lim, riem):
     return dict(reconstructor=recon, slope_limiter=lim, riemann_solver=riem)
 
 
+@pytest.mark.parametrize("mu", [0.0, 0.02])
 @pytest.mark.parametrize("riem", ["hll", "rusanov"])
 @pytest.mark.parametrize("recon,lim", LIMITERS)
-def test_residual_against_oracle(recon, lim, riem):
+def test_residual_against_oracle(recon, lim, riem, mu):
     rng = np.random.default_rng(21)
+    prm = dict(PRM, dynamic_viscosity=mu)
     U = to_fp32(random_ns_state(tuple(x + 2 for x in N), rng))
-    ref = O.ns_rhs(U, O.Geometry("cartesian", CFG), PRM, _osch(recon, lim, riem))
-    for ty, z in ((0, 0), (8, 5)):
-        sim = _sim(recon, lim, riem, [["periodic"] * 6] * 5, tile_ty=ty, zchunk=z)
+    ref = O.ns_rhs(U, O.Geometry("cartesian", CFG), prm, _osch(recon, lim, riem))
+    for ty, z in ((0, 0), (ALT[mu], 5)):
+        sim = _sim(recon, lim, riem, [["periodic"] * 6] * 5, tile_ty=ty, zchunk=z, prm=prm)
         sim.upload(U)
         e = rel_linf(sim.residual(), ref)
         sim.close()
-        assert e <= 2e-6, (recon, lim, riem, ty, z, e)
+        assert e <= 2e-6, (recon, lim, riem, mu, ty, z, e)
 
 
+@pytest.mark.parametrize("mu", [0.0, 0.02])
 @pytest.mark.parametrize("integrator", ["euler_explicit", "rk3", "rk3_ssp", "rk4"])
 @pytest.mark.parametrize("recon,lim,riem", [("muscl", "minmod", "hll"), ("muscl", "van_leer", "rusanov"),
                                             ("muscl", "monotonized_central", "hll"),
                                             ("piecewise_constant", None, "rusanov")])
-def test_walled_steps_against_oracle(recon, lim, riem, integrator):
+def test_walled_steps_against_oracle(recon, lim, riem, integrator, mu):
     rng = np.random.default_rng(22)
+    prm = dict(PRM, dynamic_viscosity=mu)
     U = to_fp32(random_ns_state(tuple(x + 2 for x in N), rng))
     Uo = U.copy()
-    dts = O.run("navier_stokes", Uo, PRM, O.Geometry("cartesian", CFG), _osch(recon, lim, riem), oracle_bcs(WALLS),
+    dts = O.run("navier_stokes", Uo, prm, O.Geometry("cartesian", CFG), _osch(recon, lim, riem), oracle_bcs(WALLS),
                 integrator, 0.3, 4)
     outs = []
-    for ty, z in ((0, 0), (8, 4), (16, 3)):
-        sim = _sim(recon, lim, riem, WALLS, tile_ty=ty, zchunk=z, integrator=integrator)
+    for ty, z in ((0, 0), (ALT[mu], 4), (0, 3)):
+        sim = _sim(recon, lim, riem, WALLS, tile_ty=ty, zchunk=z, integrator=integrator, prm=prm)
         sim.upload(U)
         sim.set_time(0.0, math.inf, 0.3)
         sim.step(4)
@@ -81,20 +87,22 @@ def test_walled_steps_against_oracle(recon, lim, riem, integrator):
         outs.append(sim.download())
         sim.close()
         e = rel_l2(outs[-1][I3], Uo[I3])
-        assert e <= 1e-5, (recon, lim, riem, integrator, ty, z, e)
+        assert e <= 1e-5, (recon, lim, riem, integrator, mu, ty, z, e)
     assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
 
 
+@pytest.mark.parametrize("mu", [0.0, 0.02])
 @pytest.mark.parametrize("n", [(45, 27, 1), (33, 17, 2), (7, 5, 3)])
-def test_one_plane_and_thin_grids(n):
+def test_one_plane_and_thin_grids(n, mu):
     """nx3 = 1 and nx3 = 2 grids (the z-march has one or two output planes and
     reads ghost planes on both sides) and a grid narrower than one tile."""
     cfg = dict(CFG, nx1=n[0], nx2=n[1], nx3=n[2])
     rng = np.random.default_rng(sum(n))
     U = to_fp32(random_ns_state(tuple(x + 2 for x in n), rng))
     kinds = [["periodic"] * 4 + ["neumann", "neumann"]] * 5
-    ref = O.ns_rhs(U, O.Geometry("cartesian", cfg), PRM, _osch("muscl", "van_leer", "hll"))
-    sim = _sim("muscl", "van_leer", "hll", kinds, cfg=cfg)
+    prm = dict(PRM, dynamic_viscosity=mu)
+    ref = O.ns_rhs(U, O.Geometry("cartesian", cfg), prm, _osch("muscl", "van_leer", "hll"))
+    sim = _sim("muscl", "van_leer", "hll", kinds, cfg=cfg, prm=prm)
     sim.upload(U)
     e = rel_linf(sim.residual(), ref)
     sim.close()

@@ -1,6 +1,6 @@
-"""The second block shape of the float32 kernels (4-row tiles for viscous
-navier_stokes; 8 rows against the default 16 for the register-blocked inviscid
-cartesian navier_stokes and piecewise-constant heat kernels): its residual
+"""The second block shape of the register-blocked float32 kernels (4 rows
+against the default 8 for viscous cartesian navier_stokes; 8 rows against the
+default 16 for inviscid navier_stokes and piecewise-constant heat): its residual
 matches the oracle on a grid of many partial tiles, its steps are bitwise equal
 to the default shape's (a cell's arithmetic does not depend on the tile it sits
 in), and the autotuner picks one of the two shapes and leaves the state as it
