@@ -161,9 +161,12 @@ int fvm_clear_status(fvm_handle* h);
 /* Limit (ns, default 2e9) of every wait of the stage kernels for a plane of
  * the TMA ring or a staged tile.  A wait that runs out sets FVM_ST_TIMEOUT;
  * the block then waits (up to 1 s per copy) for the copies it has in flight
- * and returns, so the context stays usable.  New: the reference has no device
- * waits (its only observability is the print of src/solver.py:147). */
-int fvm_set_wait_limit(fvm_handle* h, unsigned long long data_wait_ns);
+ * and returns, so the context stays usable.  never_complete != 0 is for tests
+ * of that path: every ring copy then expects 16 bytes more than it delivers,
+ * so no ring wait can complete and each runs out at the limit (the wait for
+ * copies in flight is then 0.1 s).  New: the reference has no device waits
+ * (its only observability is the print of src/solver.py:147). */
+int fvm_set_wait_limit(fvm_handle* h, unsigned long long data_wait_ns, int never_complete);
 
 /* Per-launch device time of the stage kernels (ms, CUDA events on the handle's
  * stream) over n_steps un-captured steps; fills per-stage totals. */

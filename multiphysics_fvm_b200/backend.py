@@ -285,10 +285,13 @@ class Simulation:
     def clear_status(self):
         L.check(self._lib.fvm_clear_status(self._h), "fvm_clear_status")
 
-    def set_wait_limit(self, ns: int):
+    def set_wait_limit(self, ns: int, never_complete: bool = False):
         """Limit (ns) of each wait of the stage kernels for a TMA plane; a wait
-        that runs out sets the timeout status bit and the step returns."""
-        L.check(self._lib.fvm_set_wait_limit(self._h, C.c_ulonglong(int(ns))), "fvm_set_wait_limit")
+        that runs out sets the timeout status bit and the step returns.
+        ``never_complete`` (tests of that path) makes every ring copy expect
+        more bytes than it delivers, so every ring wait runs out."""
+        L.check(self._lib.fvm_set_wait_limit(self._h, C.c_ulonglong(int(ns)), 1 if never_complete else 0),
+                "fvm_set_wait_limit")
 
     def autotune(self):
         """Choose the z-march depth by timing candidates (state restored); returns (zchunk, ms/step)."""

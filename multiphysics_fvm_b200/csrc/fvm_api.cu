@@ -122,6 +122,8 @@ struct fvm_handle {
   CUtensorMap smap{}, amap{};  // staged U0 / accumulator tiles of the float32 cartesian NS kernel
   bool legacy = false;         // batch member: runs the batched (tile-list) kernels
   unsigned long long wait_ns = 2000000000ull;  // limit of each wait for a TMA plane
+  unsigned long long drain_ns = 1000000000ull; // limit of the wait for copies in flight after a timeout
+  unsigned extra_tx = 0;                       // test of the timeout path (fvm_set_wait_limit)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   double max_inv_l2 = 0.0, const_rate = 0.0;
   int zchunk = 64;
@@ -150,6 +152,9 @@ bool heat_pc_desc(const fvm_desc& d) {
   return d.precision == FVM_FP32 && d.physics == FVM_HEAT && d.reconstructor == FVM_PIECEWISE_CONSTANT;
 }
 bool heat_pc_kernel(const fvm_handle* h) { return !h->legacy && heat_pc_desc(h->d); }
+bool mx_strip_desc(const fvm_desc& d) { return d.precision == FVM_FP32 && d.physics == FVM_MAXWELL; }
+// kernels whose stage combination reads TMA-staged U0 / accumulator tiles
+bool staged_kernel(const fvm_handle* h) { return strip_kernel(h) || mx_strip_desc(h->d); }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -209,7 +214,7 @@ int make_tmaps(fvm_handle* h) {
   const int rows = h->tile_ty + 2 * tile_halo(h->d);
   for (int b = 0; b < 3; ++b)
     if (int rc = make_tmap(h, b, rows)) return rc;
-  if (strip_kernel(h)) {
+  if (staged_kernel(h)) {
     if (int rc = make_stage_tmap(h, &h->smap, h->U[0], h->tile_ty)) return rc;
     if (h->acc)
       if (int rc = make_stage_tmap(h, &h->amap, h->acc, h->tile_ty)) return rc;
@@ -255,11 +260,12 @@ int default_tile_ty(const fvm_desc& d) {
   if (strip_desc(d)) return visc ? NS_STRIP_VISC_TY : NS_STRIP_TY;
   if (heat_pc_desc(d)) return HEAT_PC_TY;
   if (d.physics == FVM_HEAT) return HEAT_TY;
-  if (d.physics == FVM_MAXWELL) return f64 ? maxwell_tile_ty<double>() : maxwell_tile_ty<float>();
+  if (d.physics == FVM_MAXWELL) return f64 ? maxwell_tile_ty<double>() : MX_STRIP_TY;
   if (f64) return visc ? ns_tile_ty<double, true>() : ns_tile_ty<double, false>();
   return visc ? ns_tile_ty<float, true>() : ns_tile_ty<float, false>();
 }
 int alt_tile_ty(const fvm_desc& d) {
+  if (mx_strip_desc(d)) return MX_STRIP_TY_ALT;
   if (d.precision == FVM_FP64 || d.physics == FVM_MAXWELL) return default_tile_ty(d);
   if (heat_pc_desc(d)) return HEAT_PC_TY_ALT;
   if (d.physics == FVM_HEAT) return HEAT_TY_ALT;
@@ -347,6 +353,8 @@ void fill_common(fvm_handle* h, const StageDef& sd, bool rhs_only, P& p) {
   p.status = h->status;
   p.zchunk = h->zchunk;
   p.wait_ns = h->wait_ns;
+  p.drain_ns = h->drain_ns;
+  p.extra_tx = h->extra_tx;
 }
 
 // x3 fluxes cancel exactly on a one-plane grid whose x3 ghosts copy the plane
@@ -415,6 +423,15 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
     p.chi_b = d.params[4];
     p.chi_d = d.params[5];
     p.c = 1 / std::sqrt(d.params[0] * d.params[1]);
+    if constexpr (std::is_same<Real, float>::value) {
+      MxStripSource src;
+      src.tmap = h->tmap[sd.in];
+      src.u0map = h->smap;
+      src.accmap = h->amap;
+      src.p = p;
+      const int nbuf = (needs_u0_host(sd) ? 1 : 0) + (sd.mode == MODE_FINAL || sd.accmode == ACC_ADD ? 1 : 0);
+      return launch_mx_strip(kernel_limiter(d), d.coords, src, h->tile_ty, nbuf, h->stream, nsm);
+    }
     return launch_maxwell<Real>(kernel_limiter(d), d.riemann, d.coords, h->tmap[sd.in], p, h->stream, nsm);
   }
   const bool visc = d.params[1] != 0.0;
@@ -1002,11 +1019,16 @@ int fvm_clear_status(fvm_handle* h) {
   return FVM_OK;
 }
 
-int fvm_set_wait_limit(fvm_handle* h, unsigned long long data_wait_ns) {
+int fvm_set_wait_limit(fvm_handle* h, unsigned long long data_wait_ns, int never_complete) {
   if (!h) return fail(FVM_E_INVALID, "null handle");
   if (data_wait_ns == 0) return fail(FVM_E_INVALID, "fvm_set_wait_limit: the limit must be > 0 ns");
   FVM_CK(cudaStreamSynchronize(h->stream));
   h->wait_ns = data_wait_ns;
+  // test switch: every ring copy expects 16 bytes more than it delivers, so
+  // no ring wait completes; the copies themselves land within microseconds,
+  // so the wait for them after a timeout needs only a short limit
+  h->extra_tx = never_complete ? 16u : 0u;
+  h->drain_ns = never_complete ? 100000000ull : 1000000000ull;
   for (auto& g : h->graph)  // the captured steps hold the old limit
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return FVM_OK;

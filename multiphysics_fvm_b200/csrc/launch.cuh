@@ -8,6 +8,7 @@
 #include "stage_heat.cuh"
 #include "stage_heat_pc.cuh"
 #include "stage_maxwell.cuh"
+#include "stage_maxwell_strip.cuh"
 
 namespace fvm {
 
@@ -379,4 +380,31 @@ cudaError_t launch_maxwell(int lim, int riem, int coord, const CUtensorMap& map,
   return launch_maxwell_coord<Real, COORD_SPH>(lim, riem, map, p, s, nsm);
 }
 
+// Float32 Maxwell (stage_maxwell_strip.cuh): TY = 8 (2 rows per thread, 4
+// output warps) or 16 (4 rows per thread, 4 output warps).
+constexpr int MX_STRIP_TY = 8, MX_STRIP_TY_ALT = 16;
+
+template <int LIM, int COORD, int TY>
+cudaError_t launch_mx_strip_ty(const MxStripSource& src, int nbuf, cudaStream_t s, int nsm) {
+  constexpr int R = TY == 8 ? 2 : 4, NW = TY / R;
+  using C = MxStripCfg<R, NW>;
+  auto kern = mx_strip_kernel<LIM, COORD, R, NW, TY == 8 ? 3 : 2>;
+  static int bps[3] = {0, 0, 0};
+  if (bps[0] == 0 || nsm < 0) {
+    for (int nb = 0; nb < 3; ++nb) {
+      cudaError_t e = prepare_kernel(kern, C::NT, C::bytes(nb), &bps[nb]);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (nsm < 0) return cudaSuccess;
+  const long long ntiles = (long long)src.p.ntx * src.p.nty * src.p.nzc;
+  if (ntiles <= 0) return cudaSuccess;
+  const int grid = (int)(ntiles < (long long)bps[nbuf] * nsm ? ntiles : (long long)bps[nbuf] * nsm);
+  kern<<<grid, C::NT, C::bytes(nbuf), s>>>(src);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mx_strip(int lim, int coord, MxStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm);
+
 }  // namespace fvm
+

@@ -29,6 +29,8 @@ struct MaxwellParams {
   unsigned* status;
   int zchunk, ntx, nty, nzc;
   unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
+  unsigned long long drain_ns;  // limit of the wait for copies in flight after a timeout (ns)
+  unsigned extra_tx;  // test of the timeout path: bytes a ring copy never delivers (0 normally)
 };
 
 template <typename Real, int TY>
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
       const int s = pmod(pl, C::NSLOT);
       pending |= 1u << s;
       fence_proxy_async();
-      mbar_arrive_expect_tx(&bars[s], C::TX_BYTES);
+      mbar_arrive_expect_tx(&bars[s], C::TX_BYTES + p.extra_tx);
       tma_load_4d(&uring[s * C::SLOT], &tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
     };
     if (tid == 0) issue(Pfirst);
@@ -459,7 +461,7 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
   if constexpr (STAGED) cp_async_wait_all();  // none left in flight at exit
   if (!ok && tid == 0)
     for (int s = 0; s < C::NSLOT; ++s)
-      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 1000000000ull);
+      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.drain_ns);
 }
 
 }  // namespace fvm

@@ -35,6 +35,8 @@ struct NsParams {
   int zchunk, ntx, nty, nzc;
   int flat;  // nx3 == 1 with x3 ghosts equal to the plane: x3 fluxes cancel, no z-march
   unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
+  unsigned long long drain_ns;  // limit of the wait for copies in flight after a timeout (ns)
+  unsigned extra_tx;  // test of the timeout path: bytes a ring copy never delivers (0 normally)
 };
 
 // Tile sources: one grid (params + tensor map in kernel parameter space) or a
@@ -264,7 +266,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       const int s = pmod(pl, C::NSLOT);
       pending |= 1u << s;
       fence_proxy_async();
-      mbar_arrive_expect_tx(&bars[s], C::TX_BYTES);
+      mbar_arrive_expect_tx(&bars[s], C::TX_BYTES + p.extra_tx);
       tma_load_4d(&uring[s * C::SLOT], tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
     };
     // planes needed by the first step plus one of prefetch
@@ -745,7 +747,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
   // On a timeout, wait (bounded) for every load this block may still have in flight.
   if (!ok && tid == 0) {
     for (int s = 0; s < C::NSLOT; ++s)
-      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 1000000000ull);
+      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.drain_ns);
   }
 }
 

@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(NsStripViscCfg<R, NW>::NT, MINB)
       const int s = pmod(pl, C::NSLOT);
       pending |= 1u << s;
       fence_proxy_async();
-      mbar_arrive_expect_tx(&bars[s], C::TX_BYTES);
+      mbar_arrive_expect_tx(&bars[s], C::TX_BYTES + p.extra_tx);
       tma_load_4d(&uring[s * C::SLOT], &src.tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
     };
     if (tid == 0)
@@ -548,7 +548,7 @@ __global__ void __launch_bounds__(NsStripViscCfg<R, NW>::NT, MINB)
   }
   if (!ok && tid == 0) {
     for (int s = 0; s < C::NBAR; ++s)
-      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, 1000000000ull);
+      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.drain_ns);
   }
 }
 

@@ -2,9 +2,10 @@
 
 Every wait of a stage kernel for a TMA plane (or a staged U0 / accumulator
 tile) is bounded by the handle's wait limit (fvm_set_wait_limit, default 2 s).
-Here the limit is set to 1 ns, far below the latency of any copy, so the first
-waits of the step run out: the kernel must set FVM_ST_TIMEOUT, wait (bounded)
-for its own copies in flight and return.  The same handle, with the default
+Here every ring copy is made to expect 16 bytes more than it delivers, so no
+ring wait can complete (a wait on something that never happens), and the limit
+is 1 ms: the kernel must set FVM_ST_TIMEOUT, wait (bounded) for its own copies
+in flight and return.  The same handle, with the default
 limit restored and the state uploaded again, then runs clean steps whose result
 is bitwise equal to a fresh handle's, so the context stayed usable.  No wait is
 left without a limit and nothing traps.
@@ -19,23 +20,25 @@ from tests.helpers import bcs_dict, random_ns_state
 pytestmark = pytest.mark.gpu
 
 CASES = [
-    # (physics, precision, viscosity): the register-blocked float32 kernel, the
-    # general kernel (float64, viscous float32), heat and Maxwell
-    ("navier_stokes", "fp32", 0.0),
-    ("navier_stokes", "fp64", 0.0),
-    ("navier_stokes", "fp32", 1e-3),
-    ("heat", "fp32", None),
-    ("maxwell", "fp32", None),
+    # (physics, precision, viscosity, reconstructor): the register-blocked
+    # float32 kernels (inviscid and viscous NS, piecewise-constant heat,
+    # Maxwell) and the general ones (float64 NS, MUSCL heat)
+    ("navier_stokes", "fp32", 0.0, "muscl"),
+    ("navier_stokes", "fp32", 1e-3, "muscl"),
+    ("navier_stokes", "fp64", 0.0, "muscl"),
+    ("heat", "fp32", None, "muscl"),
+    ("heat", "fp32", None, "piecewise_constant"),
+    ("maxwell", "fp32", None, "muscl"),
 ]
 
 
-def _make(physics, precision, mu):
+def _make(physics, precision, mu, recon):
     from multiphysics_fvm_b200.backend import Simulation
     from multiphysics_fvm_b200.numerics import (diffusive_solvers, reconstructors, riemann_solvers,
                                                 slope_limiters, time_integrators)
     n = (48, 40, 36)
     cfg = dict(x1_min=0, x1_max=1, x2_min=0, x2_max=0.8, x3_min=0, x3_max=0.7, nx1=n[0], nx2=n[1], nx3=n[2])
-    sch = {"reconstructor": reconstructors.muscl, "slope_limiter": slope_limiters.minmod,
+    sch = {"reconstructor": getattr(reconstructors, recon), "slope_limiter": slope_limiters.minmod,
            "riemann_solver": riemann_solvers.hll, "diffusive_solver": diffusive_solvers.centered}
     rng = np.random.default_rng(12)
     sh = tuple(x + 2 for x in n)
@@ -59,14 +62,14 @@ def _make(physics, precision, mu):
     return make, U
 
 
-@pytest.mark.parametrize("physics,precision,mu", CASES)
-def test_short_wait_limit_reports_timeout_and_context_survives(physics, precision, mu):
+@pytest.mark.parametrize("physics,precision,mu,recon", CASES)
+def test_short_wait_limit_reports_timeout_and_context_survives(physics, precision, mu, recon):
     from multiphysics_fvm_b200._lib import ST_TIMEOUT
-    make, U = _make(physics, precision, mu)
+    make, U = _make(physics, precision, mu, recon)
     sim = make()
     sim.upload(U)
     sim.set_time(0.0, math.inf, 0.4)
-    sim.set_wait_limit(1)  # 1 ns: the waits give up
+    sim.set_wait_limit(1_000_000, never_complete=True)  # the ring waits cannot complete
     sim.step(1)  # returns: no hang, no fault
     st = sim.status()
     assert st & ST_TIMEOUT, f"status {st:#x}"
