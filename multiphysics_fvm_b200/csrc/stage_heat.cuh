@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
   }
   if (!ok && tid == 0)
     for (int s = 0; s < C::NSLOT; ++s)
-      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.drain_ns);
+      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, src.params(0).drain_ns);
 }
 
 }  // namespace fvm

@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
   // On a timeout, wait (bounded) for every load this block may still have in flight.
   if (!ok && tid == 0) {
     for (int s = 0; s < C::NSLOT; ++s)
-      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.drain_ns);
+      if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, src.params(0).drain_ns);
   }
 }
 
