@@ -1,6 +1,9 @@
 """Batched persistent launch (many uneven grids, one launch per kernel
 specialisation and stage, per-grid CFL dt) against the same grids advanced one
-at a time, and the autotuner's state restoration."""
+at a time, and the autotuner's state restoration.  Batched grids run the
+tile-list kernels and single float32 grids the register-blocked ones, whose
+float32 rounding differs: the states agree to relative L2 <= 1e-5 after 6
+steps and the simulated times to 1e-6."""
 import numpy as np
 import pytest
 
@@ -26,9 +29,9 @@ def test_batch_matches_single_grids():
         sim.set_time(0.0, float("inf"), s["time_config"]["CFL"])
         sim.step(6)
         a, b = batch[i].download(), sim.download()
-        assert np.array_equal(a, b), (i, rel_l2(a, b))
+        assert rel_l2(a, b) <= 1e-5, (i, rel_l2(a, b))
         assert batch[i].time()[1] == 6 and batch[i].status() == 0
-        assert batch[i].time()[0] == sim.time()[0]  # per-grid dt
+        assert abs(batch[i].time()[0] - sim.time()[0]) <= 1e-6 * sim.time()[0]  # per-grid dt
         sim.close()
     dts = {batch[i].time()[2] for i in range(len(setups))}
     assert len(dts) > 1  # grids advanced with different time steps
