@@ -157,14 +157,15 @@ cudaError_t launch_ns(int lim, int riem, int coord, bool visc, const CUtensorMap
 
 // ------------------------------------------------ float32 cartesian NS ----
 // Register-blocked stage kernel (stage_ns_strip.cuh) for float32 inviscid
-// cartesian grids: 4 rows per thread, TY = 16 (4 output warps) or 8 (2).
+// cartesian grids: TY = 16 (4 rows per thread, 4 output warps, 2 blocks/SM) or
+// 8 (2 rows per thread, 4 output warps, 3 blocks/SM at 128 registers).
 constexpr int NS_STRIP_TY = 16, NS_STRIP_TY_ALT = 8;
 
 template <int LIM, int RIEM, int TY>
 cudaError_t launch_ns_strip_ty(const NsStripSource& src, int nbuf, cudaStream_t s, int nsm) {
-  constexpr int R = 4, NW = TY / R;
+  constexpr int R = TY == 16 ? 4 : 2, NW = TY / R;
   using C = NsStripCfg<R, NW>;
-  auto kern = ns_strip_kernel<LIM, RIEM, R, NW, TY == 16 ? 2 : 4>;
+  auto kern = ns_strip_kernel<LIM, RIEM, R, NW, TY == 16 ? 2 : 3>;
   static int bps[3] = {0, 0, 0};
   if (bps[0] == 0 || nsm < 0) {
     // occupancy with 0, 1 and 2 staged tiles; the attribute ends at the largest

@@ -26,7 +26,7 @@
 //      K+1/2; the left state and the flux at K-1/2 are carried in registers;
 //   6. divergence with the inverse cell lengths, gravity, stage combination
 //      with U0 / acc from shared memory, coalesced stores;
-//   7. one block barrier (after it, plane K's slot is free).
+//   7. one block barrier per step (after it, plane K's slot is free).
 // Face values are the reference's: MUSCL slopes limiter(f_i - f_i-1,
 // f_i+1 - f_i) (zero in ghost cells, reconstructors.py:120-132), states
 // f +- s/2, Euler flux from the face U and the reconstructed face P, HLL or
@@ -358,25 +358,25 @@ __global__ void __launch_bounds__(NsStripCfg<R, NW>::NT, MINB)
         }
       }
       // ------------------------------------------------------------ 3 ----
-      {
-        bool got = true;
-        for (int pl = (K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
-          const int s = pmod(pl, C::NSLOT);
-          const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
-          if (g) {
-            phase_bits ^= 1u << s;
-            if (tid == 0) pending &= ~(1u << s);
-          }
-          got = g;
+      // Every thread waits for the plane itself; nothing read after the wait
+      // was written by another thread in this step, so the block needs no
+      // barrier here.  A thread whose wait ran out skips the rest of the step
+      // and the barrier at its end takes the block out.
+      bool got = true;
+      for (int pl = (K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
+        const int s = pmod(pl, C::NSLOT);
+        const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
+        if (g) {
+          phase_bits ^= 1u << s;
+          if (tid == 0) pending &= ~(1u << s);
         }
-        if (!__syncthreads_and(got)) {
-          if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
-          ok = false;
-          break;
-        }
+        got = g;
       }
-      bool step_ok = true;
-      if (is_out) {
+      if (!got) atomicOr(p.status, ST_TMA_TIMEOUT);
+      bool step_ok = got;
+      if (!got) {
+        // skip to the barrier
+      } else if (is_out) {
         // ------------------------------------------------------------ 4 ----
         float pnew[R];
 #pragma unroll
@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(NsStripCfg<R, NW>::NT, MINB)
               if (tid == 0) pending &= ~(1u << C::NSLOT);
             }
           }
-          step_ok = staged_ok;
+          step_ok = step_ok && staged_ok;
           unsigned bad = staged_ok ? 0u : ST_TMA_TIMEOUT;
           const int jb = y0 + w * R;
 #pragma unroll

@@ -420,6 +420,8 @@ __global__ void __launch_bounds__(NsStripViscCfg<R, NW>::NT, MINB)
         }
       }
       // ------------------------------------------------------------ 3 ----
+      // each thread waits for the plane itself; the barrier after v of the
+      // new plane also takes the block out if any wait ran out
       {
         bool got = true;
         for (int pl = (K == Kfirst ? Kfirst : K + 3); pl <= K + 3; ++pl) {
@@ -431,6 +433,7 @@ __global__ void __launch_bounds__(NsStripViscCfg<R, NW>::NT, MINB)
           }
           got = g;
         }
+        if (K != Kfirst && got) velocity(K + 3);
         if (!__syncthreads_and(got)) {
           if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
           ok = false;
@@ -448,9 +451,9 @@ __global__ void __launch_bounds__(NsStripViscCfg<R, NW>::NT, MINB)
         float skip[R][4];
         closure_plane(K + 1, skip);
         __syncthreads();
+        velocity(K + 3);
+        __syncthreads();
       }
-      velocity(K + 3);
-      __syncthreads();
       // ------------------------------------------------------------ 4 ----
       closure_plane(K + 2, own);
       bool step_ok = true;
