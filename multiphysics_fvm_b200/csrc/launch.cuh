@@ -157,15 +157,15 @@ cudaError_t launch_ns(int lim, int riem, int coord, bool visc, const CUtensorMap
 
 // ------------------------------------------------ float32 cartesian NS ----
 // Register-blocked stage kernel (stage_ns_strip.cuh) for float32 inviscid
-// cartesian grids: TY = 16 (4 rows per thread, 4 output warps, 2 blocks/SM) or
-// 8 (2 rows per thread, 4 output warps, 3 blocks/SM at 128 registers).
-constexpr int NS_STRIP_TY = 16, NS_STRIP_TY_ALT = 8;
+// cartesian grids, 2 rows per thread: TY = 8 (4 output warps, 4 blocks/SM at
+// 96 registers) or 16 (8 output warps, 2 blocks/SM).
+constexpr int NS_STRIP_TY = 8, NS_STRIP_TY_ALT = 16;
 
 template <int LIM, int RIEM, int TY>
 cudaError_t launch_ns_strip_ty(const NsStripSource& src, int nbuf, cudaStream_t s, int nsm) {
-  constexpr int R = TY == 16 ? 4 : 2, NW = TY / R;
+  constexpr int R = 2, NW = TY / R;
   using C = NsStripCfg<R, NW>;
-  auto kern = ns_strip_kernel<LIM, RIEM, R, NW, TY == 16 ? 2 : 3>;
+  auto kern = ns_strip_kernel<LIM, RIEM, R, NW, TY == 8 ? 4 : 2>;
   static int bps[3] = {0, 0, 0};
   if (bps[0] == 0 || nsm < 0) {
     // occupancy with 0, 1 and 2 staged tiles; the attribute ends at the largest
@@ -195,8 +195,9 @@ cudaError_t launch_ns_strip_lr(NsStripSource& src, int ty, int nbuf, cudaStream_
 cudaError_t launch_ns_strip(int lim, int riem, NsStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm);
 
 // Viscous float32 cartesian grids (stage_ns_strip_visc.cuh): 2 rows per
-// thread, TY = 8 (4 output warps) or 4 (2).
-constexpr int NS_STRIP_VISC_TY = 8, NS_STRIP_VISC_TY_ALT = 4;
+// thread, TY = 8 (4 output warps).  It is the second block shape of these
+// grids; the default one runs the general kernel (stage_ns.cuh).
+constexpr int NS_STRIP_VISC_TY = 8;
 
 template <int LIM, int RIEM, int TY>
 cudaError_t launch_ns_strip_visc_ty(const NsStripSource& src, int nbuf, cudaStream_t s, int nsm) {
@@ -224,7 +225,7 @@ cudaError_t launch_ns_strip_visc_lr(NsStripSource& src, int ty, int nbuf, cudaSt
   p.ntx = (p.lay.nx + 31) / 32;
   p.nty = (p.lay.ny + ty - 1) / ty;
   p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
-  if (ty == NS_STRIP_VISC_TY_ALT) return launch_ns_strip_visc_ty<LIM, RIEM, NS_STRIP_VISC_TY_ALT>(src, nbuf, s, nsm);
+  (void)ty;
   return launch_ns_strip_visc_ty<LIM, RIEM, NS_STRIP_VISC_TY>(src, nbuf, s, nsm);
 }
 

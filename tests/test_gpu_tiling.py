@@ -1,6 +1,7 @@
-"""The second block shape of the register-blocked float32 kernels (4 rows
-against the default 8 for viscous cartesian navier_stokes; 8 rows against the
-default 16 for inviscid navier_stokes and piecewise-constant heat): its residual
+"""The second block shape of the float32 kernels (for viscous cartesian
+navier_stokes the 8-row register-blocked kernel against the default 6-row
+general one, 16 rows against 8 for inviscid navier_stokes, 8 against 16 for
+piecewise-constant heat): its residual
 matches the oracle on a grid of many partial tiles, its steps are bitwise equal
 to the default shape's (a cell's arithmetic does not depend on the tile it sits
 in), and the autotuner picks one of the two shapes and leaves the state as it
@@ -11,7 +12,7 @@ import numpy as np
 import pytest
 
 from oracle import fvm_oracle as O
-from tests.helpers import bcs_dict, oracle_schemes, random_ns_state, rel_linf, schemes_from_case, to_fp32
+from tests.helpers import bcs_dict, oracle_schemes, random_ns_state, rel_l2, rel_linf, schemes_from_case, to_fp32
 
 pytestmark = pytest.mark.gpu
 
@@ -46,12 +47,13 @@ def _state(c, rng):
     return to_fp32(random_ns_state(sh, rng))
 
 
-ALT_ROWS = [4, 8, 8]
+ALT_ROWS = [8, 16, 8]
+SAME_KERNEL = [False, True, True]  # viscous: the two shapes are two kernels
 
 
-@pytest.mark.parametrize("c,prm,alt", [cp + (a,) for cp, a in zip(CASES, ALT_ROWS)],
+@pytest.mark.parametrize("c,prm,alt,same", [cp + (a, sk) for cp, a, sk in zip(CASES, ALT_ROWS, SAME_KERNEL)],
                          ids=["ns_viscous", "ns_inviscid", "heat"])
-def test_second_block_shape(c, prm, alt):
+def test_second_block_shape(c, prm, alt, same):
     c = dict(c, coords="cartesian", grid=CFG)
     rng = np.random.default_rng(13)
     U = _state(c, rng)
@@ -67,7 +69,10 @@ def test_second_block_shape(c, prm, alt):
         sim.step(3)
         assert sim.status() == 0
         outs[ty] = sim.download()
-    assert np.array_equal(outs[0], outs[alt])
+    if same:
+        assert np.array_equal(outs[0], outs[alt])
+    else:  # two kernels with their own float32 rounding
+        assert rel_l2(outs[0], outs[alt]) <= 1e-6
 
 
 def test_autotune_chooses_a_shape_and_restores_the_state():
