@@ -157,15 +157,15 @@ cudaError_t launch_ns(int lim, int riem, int coord, bool visc, const CUtensorMap
 
 // ------------------------------------------------ float32 cartesian NS ----
 // Register-blocked stage kernel (stage_ns_strip.cuh) for float32 inviscid
-// cartesian grids, 2 rows per thread: TY = 8 (4 output warps, 4 blocks/SM at
-// 96 registers) or 16 (8 output warps, 2 blocks/SM).
+// cartesian grids, 2 rows per thread: TY = 8 (4 output warps, 3 blocks/SM at
+// 128 registers) or 16 (8 output warps, 2 blocks/SM).
 constexpr int NS_STRIP_TY = 8, NS_STRIP_TY_ALT = 16;
 
 template <int LIM, int RIEM, int TY>
 cudaError_t launch_ns_strip_ty(const NsStripSource& src, int nbuf, cudaStream_t s, int nsm) {
   constexpr int R = 2, NW = TY / R;
   using C = NsStripCfg<R, NW>;
-  auto kern = ns_strip_kernel<LIM, RIEM, R, NW, TY == 8 ? 4 : 2>;
+  auto kern = ns_strip_kernel<LIM, RIEM, R, NW, TY == 8 ? 3 : 2>;
   static int bps[3] = {0, 0, 0};
   if (bps[0] == 0 || nsm < 0) {
     // occupancy with 0, 1 and 2 staged tiles; the attribute ends at the largest
