@@ -209,6 +209,11 @@ int fvm_batch_handle(fvm_batch* b, int i, fvm_handle** h);
 int fvm_batch_step(fvm_batch* b, int n_steps, int dt_mode);
 int fvm_batch_time_steps(fvm_batch* b, int n_steps, int dt_mode, double* ms);
 int fvm_batch_autotune(fvm_batch* b, int* best_zchunk, double* best_ms_per_step);
+/* Kernel launches per Runge-Kutta stage of one batched step.  It is 1 when every
+ * grid is float32 and either inviscid cartesian navier_stokes (one limiter and
+ * Riemann solver) or piecewise-constant heat (one coordinate system): those run
+ * as one mixed launch.  Other batches launch once per kernel specialisation. */
+int fvm_batch_launches(const fvm_batch* b, int* per_stage);
 
 /* Conserved totals sum_q(cells[q][i] * volumes[i]) in float64 with compensated
  * summation, computed without allocating any device memory.  No counterpart in

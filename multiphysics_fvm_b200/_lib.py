@@ -80,6 +80,7 @@ SIGNATURES = [
     ("fvm_batch_step", C.c_int, [_P, C.c_int, C.c_int]),
     ("fvm_batch_time_steps", C.c_int, [_P, C.c_int, C.c_int, _DP]),
     ("fvm_batch_autotune", C.c_int, [_P, C.POINTER(C.c_int), _DP]),
+    ("fvm_batch_launches", C.c_int, [_P, C.POINTER(C.c_int)]),
     ("fvm_init_kelvin_helmholtz", C.c_int, [_P, _DP, C.c_ulonglong]),
     # learned closure (include/fvm_closure.h)
     ("fvm_closure_create", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(_P)]),

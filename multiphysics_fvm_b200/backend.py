@@ -346,6 +346,13 @@ class Batch:
         L.check(self._lib.fvm_batch_size(self._b, C.byref(n), C.byref(t)), "fvm_batch_size")
         return t.value
 
+    def launches_per_stage(self) -> int:
+        """Kernel launches per Runge-Kutta stage (1 for a mixed
+        navier_stokes + heat batch that runs as one launch)."""
+        k = C.c_int()
+        L.check(self._lib.fvm_batch_launches(self._b, C.byref(k)), "fvm_batch_launches")
+        return k.value
+
     def step(self, n_steps: int = 1, fixed_dt: bool = False):
         L.check(self._lib.fvm_batch_step(self._b, int(n_steps), 1 if fixed_dt else 0), "fvm_batch_step")
 

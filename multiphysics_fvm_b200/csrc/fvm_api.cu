@@ -1149,6 +1149,8 @@ struct fvm_batch {
   struct Group {
     int physics = 0, lim = 0, riem = 0, coords = 0;
     bool visc = false;
+    bool mixed = false;  // navier_stokes (lim, riem) and heat (coords) grids in one launch
+    std::vector<int> nbuf;            // mixed: staged tiles of each stage
     std::vector<int> members;
     std::vector<void*> prm;           // device params array per stage
     std::vector<CUtensorMap*> maps;   // device tensor-map array per stage
@@ -1169,8 +1171,56 @@ struct fvm_batch {
 
 namespace {
 
+// Per-stage instance tables of the mixed group (float32 only).
+int build_mixed_arrays(fvm_batch* b, fvm_batch::Group& g) {
+  const std::vector<StageDef> st = stage_table(b->integrator);
+  for (void* x : g.prm) cudaFree(x);
+  if (g.tile_start) cudaFree(g.tile_start);
+  g.prm.clear();
+  g.nbuf.clear();
+  g.tile_start = nullptr;
+  std::vector<int> starts(1, 0);
+  for (size_t si = 0; si < st.size(); ++si) {
+    std::vector<MixedInst> mi(g.members.size());
+    for (size_t k = 0; k < g.members.size(); ++k) {
+      fvm_handle* h = b->h[g.members[k]];
+      MixedInst& m = mi[k];
+      m.tmap = h->tmap[st[si].in];
+      int tiles = 0;
+      if (h->d.physics == FVM_NAVIER_STOKES) {
+        m.kind = 0;
+        m.u0map = h->smap;
+        m.accmap = h->amap;
+        m.ns = make_ns_params<float>(h, st[si], false);
+        m.ns.ntx = (h->lay.nx + 31) / 32;
+        m.ns.nty = (h->lay.ny + MIX_NS_TY - 1) / MIX_NS_TY;
+        m.ns.nzc = (h->lay.nz + m.ns.zchunk - 1) / m.ns.zchunk;
+        tiles = m.ns.ntx * m.ns.nty * m.ns.nzc;
+      } else {
+        m.kind = 1;
+        m.heat = make_heat_params<float>(h, st[si], false);
+        m.heat.ntx = (h->lay.nx + 31) / 32;
+        m.heat.nty = (h->lay.ny + MIX_HEAT_TY - 1) / MIX_HEAT_TY;
+        m.heat.nzc = (h->lay.nz + m.heat.zchunk - 1) / m.heat.zchunk;
+        tiles = m.heat.ntx * m.heat.nty * m.heat.nzc;
+      }
+      if (si == 0) starts.push_back(starts.back() + tiles);
+    }
+    void* dev = nullptr;
+    FVM_CK(cudaMalloc(&dev, mi.size() * sizeof(MixedInst)));
+    FVM_CK(cudaMemcpy(dev, mi.data(), mi.size() * sizeof(MixedInst), cudaMemcpyHostToDevice));
+    g.prm.push_back(dev);
+    g.nbuf.push_back((needs_u0_host(st[si]) ? 1 : 0) + (st[si].mode == MODE_FINAL || st[si].accmode == ACC_ADD ? 1 : 0));
+  }
+  g.ntiles = starts.back();
+  FVM_CK(cudaMalloc(&g.tile_start, starts.size() * sizeof(int)));
+  FVM_CK(cudaMemcpy(g.tile_start, starts.data(), starts.size() * sizeof(int), cudaMemcpyHostToDevice));
+  return FVM_OK;
+}
+
 template <typename Real>
 int build_group_arrays(fvm_batch* b, fvm_batch::Group& g) {
+  if (g.mixed) return build_mixed_arrays(b, g);
   const std::vector<StageDef> st = stage_table(b->integrator);
   for (void* x : g.prm) cudaFree(x);
   for (CUtensorMap* x : g.maps) cudaFree(x);
@@ -1220,6 +1270,12 @@ int build_group_arrays(fvm_batch* b, fvm_batch::Group& g) {
 
 template <typename Real>
 cudaError_t launch_group_stage(fvm_batch* b, fvm_batch::Group& g, int si, int nsm) {
+  if (g.mixed) {
+    const int nbuf = g.nbuf[si];
+    const MixedSource src{static_cast<const MixedInst*>(g.prm[si]), g.tile_start, (int)g.members.size(),
+                          mixed_bar_offset(nbuf)};
+    return launch_mixed(g.lim, g.riem, g.coords, src, g.ntiles, nbuf, b->stream, nsm);
+  }
   if (g.physics == FVM_NAVIER_STOKES) {
     BatchSource<NsParams<Real>> src{static_cast<const NsParams<Real>*>(g.prm[si]), g.maps[si], g.tile_start,
                                     (int)g.members.size()};
@@ -1343,6 +1399,23 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
   auto bail = [&](int rc) { fvm_batch_destroy(b); return rc; };
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(FVM_E_CUDA, "stream creation failed"));
+  // One launch per stage for the whole batch when every grid is float32
+  // inviscid cartesian navier_stokes (one limiter / Riemann solver pair) or
+  // float32 piecewise-constant heat (one coordinate system).
+  bool mixed = true;
+  int mlim = -1, mriem = -1, mcoords = -1;
+  for (int i = 0; i < n && mixed; ++i) {
+    const fvm_desc& d = descs[i];
+    if (strip_desc(d) && d.params[1] == 0.0) {
+      if (mlim < 0) { mlim = kernel_limiter(d); mriem = d.riemann; }
+      mixed = kernel_limiter(d) == mlim && d.riemann == mriem;
+    } else if (heat_pc_desc(d)) {
+      if (mcoords < 0) mcoords = d.coords;
+      mixed = d.coords == mcoords;
+    } else {
+      mixed = false;
+    }
+  }
   for (int i = 0; i < n; ++i) {
     fvm_handle* h = nullptr;
     fvm_desc di = descs[i];
@@ -1350,15 +1423,27 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     int rc = fvm_create(&di, &h);
     if (rc) return bail(rc);
     b->h.push_back(h);
-    if (strip_desc(di) || heat_pc_desc(di)) {  // the tile-list kernels' shape, not the single-grid kernel's
+    if (mixed) {  // the block shapes of the mixed launch's two bodies
+      h->tile_ty = heat_pc_desc(di) ? MIX_HEAT_TY : MIX_NS_TY;
+      if ((rc = make_tmaps(h))) return bail(rc);
+    } else if (strip_desc(di) || heat_pc_desc(di)) {  // the tile-list kernels' shape, not the single-grid kernel's
       h->legacy = true;
       h->tile_ty = strip_desc(di) ? (di.params[1] != 0.0 ? ns_tile_ty<float, true>() : ns_tile_ty<float, false>())
                                   : HEAT_TY;
       if ((rc = make_tmaps(h))) return bail(rc);
     }
   }
-  // group by kernel specialisation
-  for (int i = 0; i < n; ++i) {
+  // group by kernel specialisation (one mixed group holds every grid)
+  if (mixed) {
+    b->groups.emplace_back();
+    fvm_batch::Group& g = b->groups.back();
+    g.mixed = true;
+    g.lim = std::max(mlim, 0);
+    g.riem = std::max(mriem, 0);
+    g.coords = std::max(mcoords, 0);
+    for (int i = 0; i < n; ++i) g.members.push_back(i);
+  }
+  for (int i = 0; i < n && !mixed; ++i) {
     const fvm_desc& d = descs[i];
     const int lim = kernel_limiter(d);
     const bool visc = d.physics == FVM_NAVIER_STOKES && d.params[1] != 0.0;
@@ -1415,6 +1500,14 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     b->dtg.push_back(dg);
   }
   *out = b;
+  return FVM_OK;
+}
+
+int fvm_batch_launches(const fvm_batch* b, int* per_stage) {
+  if (!b || !per_stage) return fail(FVM_E_INVALID, "null batch or output");
+  int k = 0;
+  for (auto& g : b->groups) k += g.ntiles > 0 ? 1 : 0;
+  *per_stage = k;
   return FVM_OK;
 }
 

@@ -7,6 +7,7 @@
 #include "stage_ns_strip_visc.cuh"
 #include "stage_heat.cuh"
 #include "stage_heat_pc.cuh"
+#include "stage_batch_mixed.cuh"
 #include "stage_maxwell.cuh"
 #include "stage_maxwell_strip.cuh"
 
@@ -293,6 +294,26 @@ cudaError_t launch_heat_pc_ty(const CUtensorMap& map, const HeatParams<float>& p
 }
 
 cudaError_t launch_heat_pc(int coord, const CUtensorMap& map, HeatParams<float> p, cudaStream_t s, int nsm, int ty);
+
+// Mixed batch (stage_batch_mixed.cuh): navier_stokes (limiter, Riemann
+// solver) and heat (coordinate system) tiles in one launch.
+template <int LIM, int RIEM, int HCOORD>
+cudaError_t launch_mixed_lrc(const MixedSource& src, long long ntiles, int nbuf, cudaStream_t s, int nsm) {
+  auto kern = batch_mixed_kernel<LIM, RIEM, HCOORD>;
+  static int bps[3] = {0, 0, 0};
+  if (bps[0] == 0 || nsm < 0) {
+    for (int nb = 0; nb < 3; ++nb) {
+      cudaError_t e = prepare_kernel(kern, MIX_NT, mixed_bytes(nb), &bps[nb]);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (nsm < 0 || ntiles <= 0) return cudaSuccess;
+  const int grid = (int)(ntiles < (long long)bps[nbuf] * nsm ? ntiles : (long long)bps[nbuf] * nsm);
+  kern<<<grid, MIX_NT, mixed_bytes(nbuf), s>>>(src);
+  return cudaGetLastError();
+}
+cudaError_t launch_mixed(int lim, int riem, int hcoord, const MixedSource& src, long long ntiles, int nbuf,
+                         cudaStream_t s, int nsm);
 
 template <typename Real>
 cudaError_t launch_heat(int lim, int coord, const CUtensorMap& map, const HeatParams<Real>& p0, cudaStream_t s,

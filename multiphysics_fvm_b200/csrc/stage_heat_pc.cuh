@@ -33,28 +33,18 @@ struct HeatPcCfg {
   static_assert((SLOT * 4) % 128 == 0, "TMA destinations need 128-byte alignment");
 };
 
+// One tile of the stage (all planes of its z-chunk) with the ring barriers
+// `bars` (phase bits 0..5); `phase_bits` and `pending` carry over from tile to
+// tile.  Returns false when a wait ran out: the block must stop and drain.
 template <int COORD, int R, int NW>
-__global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT)
-    heat_pc_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ HeatParams<float> p) {
+__device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const CUtensorMap* tmap, int tile,
+                                             unsigned char* smem_raw, uint64_t* bars, unsigned& phase_bits,
+                                             unsigned& pending) {
   using C = HeatPcCfg<R, NW>;
   using G = Geo<float, COORD>;
   constexpr int TX = C::TX, TY = C::TY, W = C::W, HH = C::HH;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
   float* uring = reinterpret_cast<float*>(smem_raw);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + C::NSLOT * C::SLOT * 4);
-  if (smem_u32(smem_raw) & 127u) {
-    if (threadIdx.x == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
-    return;
-  }
-  if (p.active && !*p.active) return;  // the clock passed t_end
   const int tid = threadIdx.x;
-  if (tid == 0) {
-    for (int s = 0; s < C::NSLOT; ++s) mbar_init(&bars[s], 1);
-    mbar_fence_init();
-    tma_prefetch_desc(&tmap);
-  }
-  __syncthreads();
-  unsigned phase_bits = 0, pending = 0;
   const Layout& L = p.lay;
   const Metric<float>& m = p.met;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
@@ -63,9 +53,7 @@ __global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT)
   const bool need_u0 = needs_u0<float>(p.coef) && !p.coef.u0_is_input;
   const bool need_acc = needs_acc(p.coef);
   const int w = tid >> 5, lane = tid & 31;
-  const int ntiles = p.ntx * p.nty * p.nzc;
-  bool ok = true;
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+  {
     const int x0 = (tile % p.ntx) * TX, y0 = ((tile / p.ntx) % p.nty) * TY;
     const int Z0 = 1 + (tile / (p.ntx * p.nty)) * p.zchunk;
     const int Zl = min(Z0 + p.zchunk - 1, nz);
@@ -79,7 +67,7 @@ __global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT)
       pending |= 1u << s;
       fence_proxy_async();
       mbar_arrive_expect_tx(&bars[s], C::TX_BYTES + p.extra_tx);
-      tma_load_4d(&uring[s * C::SLOT], &tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
+      tma_load_4d(&uring[s * C::SLOT], tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
     };
     if (tid == 0)
       for (int pl = Kfirst; pl <= Kfirst + C::NSLOT - 1 && pl <= Plast; ++pl) issue(pl);
@@ -143,8 +131,7 @@ __global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT)
         }
         if (!__syncthreads_and(got)) {
           if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
-          ok = false;
-          break;
+          return false;
         }
       }
       const int s2 = sK + 2 >= C::NSLOT ? sK + 2 - C::NSLOT : sK + 2;
@@ -200,6 +187,35 @@ __global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT)
       __syncthreads();  // plane K's slot is refilled at the next step
     }
   }
+  return true;
+}
+
+template <int COORD, int R, int NW>
+__global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT)
+    heat_pc_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ HeatParams<float> p) {
+  using C = HeatPcCfg<R, NW>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + C::NSLOT * C::SLOT * 4);
+  if (smem_u32(smem_raw) & 127u) {
+    if (threadIdx.x == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+    return;
+  }
+  if (p.active && !*p.active) return;  // the clock passed t_end
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < C::NSLOT; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+    tma_prefetch_desc(&tmap);
+  }
+  __syncthreads();
+  unsigned phase_bits = 0, pending = 0;
+  const int ntiles = p.ntx * p.nty * p.nzc;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    if (!heat_pc_tile<COORD, R, NW>(p, &tmap, tile, smem_raw, bars, phase_bits, pending)) {
+      ok = false;
+      break;
+    }
   if (!ok && tid == 0)
     for (int s = 0; s < C::NSLOT; ++s)
       if ((pending >> s) & 1u) mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.drain_ns);

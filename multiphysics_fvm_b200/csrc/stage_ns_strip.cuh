@@ -127,36 +127,25 @@ __device__ __forceinline__ float strip_pressure(const float* u, int PL, float gm
   return gm1 * (E - ke);
 }
 
-template <int LIM, int RIEM, int R, int NW, int MINB>
-__global__ void __launch_bounds__(NsStripCfg<R, NW>::NT, MINB)
-    ns_strip_kernel(const __grid_constant__ NsStripSource src) {
+// One tile of the stage (all planes of its z-chunk).  `bars` holds the ring
+// barriers (indices 0..2, phase bits 0..2), `gbar` the staged-tile barrier with
+// phase bit `gbit`; `phase_bits` and `pending` carry over from tile to tile.
+// Returns false when a wait ran out: the block must stop and drain.
+template <int LIM, int RIEM, int R, int NW>
+__device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CUtensorMap* tmap,
+                                              const CUtensorMap* u0map, const CUtensorMap* accmap, int tile,
+                                              unsigned char* smem_raw, uint64_t* bars, uint64_t* gbar, int gbit,
+                                              unsigned& phase_bits, unsigned& pending) {
   using C = NsStripCfg<R, NW>;
   constexpr int TX = C::TX, TY = C::TY, W = C::W, PL = C::PL, HH = C::HH, NF = C::NF, W2 = C::W2;
   constexpr int PL2 = C::PL2;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
   float* sm = reinterpret_cast<float*>(smem_raw);
   float* uring = sm + C::OFF_U;
   float* pring = sm + C::OFF_P;
   float* hl = sm + C::OFF_HL;
   float* fr = sm + C::OFF_FR;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + C::BAR_BYTES);
-  uint64_t* gbar = bars + C::NSLOT;
   float* gst = reinterpret_cast<float*>(smem_raw + C::STG_OFF_BYTES);
-  const NsParams<float>& p = src.p;
-
-  if (smem_u32(smem_raw) & 127u) {  // TMA destinations need 128-byte alignment
-    if (threadIdx.x == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
-    return;
-  }
-  if (p.active && !*p.active) return;  // the clock passed t_end: the stage is a no-op
   const int tid = threadIdx.x;
-  if (tid == 0) {
-    for (int s = 0; s < C::NBAR; ++s) mbar_init(&bars[s], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  unsigned phase_bits = 0;  // expected parity per barrier (identical in the threads that wait)
-  unsigned pending = 0;     // barriers with a copy in flight (thread 0)
   const Layout& L = p.lay;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   const float gam = float(p.gamma), gm1 = float(p.gamma) - 1.f;
@@ -169,14 +158,7 @@ __global__ void __launch_bounds__(NsStripCfg<R, NW>::NT, MINB)
   const float* gacc = gst + (need_u0 ? C::STG : 0);  // staged acc tile
   const int w = tid >> 5, lane = tid & 31;
   const bool is_out = w < NW;
-  if (tid == 0) {
-    tma_prefetch_desc(&src.tmap);
-    if (need_u0) tma_prefetch_desc(&src.u0map);
-    if (need_acc) tma_prefetch_desc(&src.accmap);
-  }
-  const int ntiles = p.ntx * p.nty * p.nzc;
-  bool ok = true;
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+  {
     const int tx_i = tile % p.ntx;
     const int ty_i = (tile / p.ntx) % p.nty;
     const int zc_i = tile / (p.ntx * p.nty);
@@ -192,7 +174,7 @@ __global__ void __launch_bounds__(NsStripCfg<R, NW>::NT, MINB)
       pending |= 1u << s;
       fence_proxy_async();
       mbar_arrive_expect_tx(&bars[s], C::TX_BYTES + p.extra_tx);
-      tma_load_4d(&uring[s * C::SLOT], &src.tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
+      tma_load_4d(&uring[s * C::SLOT], tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
     };
     // planes Kfirst .. Kfirst + 2 (the first step's)
     if (tid == 0)
@@ -225,12 +207,12 @@ __global__ void __launch_bounds__(NsStripCfg<R, NW>::NT, MINB)
       if (tid == 0) {
         if (K > Kfirst && K + 2 <= Plast) issue(K + 2);
         if (outstep && stg_bytes) {
-          pending |= 1u << C::NSLOT;
+          pending |= 1u << gbit;
           fence_proxy_async();
           mbar_arrive_expect_tx(gbar, stg_bytes);
           const int gxc = x0 + 1 + L.padx;
-          if (need_u0) tma_load_4d(gst, &src.u0map, gbar, gxc, y0 + 1, K, 0);
-          if (need_acc) tma_load_4d(gst + (need_u0 ? C::STG : 0), &src.accmap, gbar, gxc, y0 + 1, K, 0);
+          if (need_u0) tma_load_4d(gst, u0map, gbar, gxc, y0 + 1, K, 0);
+          if (need_acc) tma_load_4d(gst + (need_u0 ? C::STG : 0), accmap, gbar, gxc, y0 + 1, K, 0);
         }
       }
       float kv[R][5];
@@ -425,10 +407,10 @@ __global__ void __launch_bounds__(NsStripCfg<R, NW>::NT, MINB)
         if (outstep) {
           bool staged_ok = true;
           if (stg_bytes) {
-            staged_ok = mbar_wait_bounded(gbar, (phase_bits >> C::NSLOT) & 1u, p.wait_ns);
+            staged_ok = mbar_wait_bounded(gbar, (phase_bits >> gbit) & 1u, p.wait_ns);
             if (staged_ok) {
-              phase_bits ^= 1u << C::NSLOT;
-              if (tid == 0) pending &= ~(1u << C::NSLOT);
+              phase_bits ^= 1u << gbit;
+              if (tid == 0) pending &= ~(1u << gbit);
             }
           }
           step_ok = step_ok && staged_ok;
@@ -486,12 +468,43 @@ __global__ void __launch_bounds__(NsStripCfg<R, NW>::NT, MINB)
         }
       }
       // ------------------------------------------------------------ 7 ----
-      if (!__syncthreads_and(step_ok)) {
-        ok = false;
-        break;
-      }
+      if (!__syncthreads_and(step_ok)) return false;
     }
   }
+  return true;
+}
+
+template <int LIM, int RIEM, int R, int NW, int MINB>
+__global__ void __launch_bounds__(NsStripCfg<R, NW>::NT, MINB)
+    ns_strip_kernel(const __grid_constant__ NsStripSource src) {
+  using C = NsStripCfg<R, NW>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + C::BAR_BYTES);
+  const NsParams<float>& p = src.p;
+  if (smem_u32(smem_raw) & 127u) {  // TMA destinations need 128-byte alignment
+    if (threadIdx.x == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+    return;
+  }
+  if (p.active && !*p.active) return;  // the clock passed t_end: the stage is a no-op
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < C::NBAR; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+    tma_prefetch_desc(&src.tmap);
+    if (needs_u0<float>(p.coef) && !p.coef.u0_is_input) tma_prefetch_desc(&src.u0map);
+    if (needs_acc(p.coef)) tma_prefetch_desc(&src.accmap);
+  }
+  __syncthreads();
+  unsigned phase_bits = 0;  // expected parity per barrier (identical in the threads that wait)
+  unsigned pending = 0;     // barriers with a copy in flight (thread 0)
+  const int ntiles = p.ntx * p.nty * p.nzc;
+  bool ok = true;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    if (!ns_strip_tile<LIM, RIEM, R, NW>(p, &src.tmap, &src.u0map, &src.accmap, tile, smem_raw, bars,
+                                         bars + C::NSLOT, C::NSLOT, phase_bits, pending)) {
+      ok = false;
+      break;
+    }
   // On a timeout, wait (bounded) for every copy this block may still have in flight.
   if (!ok && tid == 0) {
     for (int s = 0; s < C::NBAR; ++s)

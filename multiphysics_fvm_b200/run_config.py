@@ -58,7 +58,7 @@ def run_batch(steps: int, warmup: int, autotune: bool, seed: int = 0):
     b.step(warmup)
     ms = b.time_steps(steps)
     st = max(b[i].status() for i in range(len(b)))
-    print(f"batch_c3 grids={len(b)} cells={cells} tiles={b.tiles()} autotune={tuned}: {ms / steps:.3f} ms/step, "
+    print(f"batch_c3 grids={len(b)} cells={cells} tiles={b.tiles()} launches/stage={b.launches_per_stage()} autotune={tuned}: {ms / steps:.3f} ms/step, "
           f"{cells * steps / (ms / 1e3):.4e} cell-updates/s, status={st}")
     return cells * steps / (ms / 1e3)
 

@@ -1,9 +1,11 @@
 """Batched persistent launch (many uneven grids, one launch per kernel
 specialisation and stage, per-grid CFL dt) against the same grids advanced one
 at a time, and the autotuner's state restoration.  Batched grids run the
-tile-list kernels and single float32 grids the register-blocked ones, whose
-float32 rounding differs: the states agree to relative L2 <= 1e-5 after 6
-steps and the simulated times to 1e-6."""
+mixed launch (the register-blocked bodies of single grids over a tile list
+covering every grid) when all grids are float32 inviscid navier_stokes or
+piecewise-constant heat, else the tile-list kernels, whose float32 rounding
+differs from the single grids' register-blocked kernels: the states agree to
+relative L2 <= 1e-5 after 6 steps and the simulated times to 1e-6."""
 import numpy as np
 import pytest
 
@@ -19,6 +21,7 @@ def test_batch_matches_single_grids():
     states = batch_mixed.initial_states(setups)
     batch = Batch(setups)
     assert batch.tiles() > 0
+    assert batch.launches_per_stage() == 1  # inviscid navier_stokes + heat: one mixed launch
     for i, U in enumerate(states):
         batch[i].upload(U)
         batch[i].set_time(0.0, float("inf"), setups[i]["time_config"]["CFL"])
@@ -36,6 +39,56 @@ def test_batch_matches_single_grids():
     dts = {batch[i].time()[2] for i in range(len(setups))}
     assert len(dts) > 1  # grids advanced with different time steps
     batch.close()
+
+
+def _advance_pair(setups, n):
+    from multiphysics_fvm_b200.backend import Batch, Simulation
+    from multiphysics_fvm_b200.setups import batch_mixed
+    states = batch_mixed.initial_states(setups)
+    batch = Batch(setups)
+    for i, U in enumerate(states):
+        batch[i].upload(U)
+        batch[i].set_time(0.0, float("inf"), setups[i]["time_config"]["CFL"])
+    batch.step(n)
+    out = []
+    for i, (s, U) in enumerate(zip(setups, states)):
+        sim = Simulation.from_setup(s)
+        sim.upload(U)
+        sim.set_time(0.0, float("inf"), s["time_config"]["CFL"])
+        sim.step(n)
+        out.append((batch[i].download(), sim.download(), batch[i].time(), sim.time(), batch[i].status()))
+        sim.close()
+    k = batch.launches_per_stage()
+    batch.close()
+    return k, out
+
+
+def test_specialised_groups_match_single_grids():
+    """A batch the mixed launch does not cover (a viscous navier_stokes grid and
+    a MUSCL heat grid) runs one launch per kernel specialisation."""
+    from multiphysics_fvm_b200.numerics import reconstructors
+    from multiphysics_fvm_b200.setups import batch_mixed
+    setups = batch_mixed.make_setups(seed=4, n_kh=3, n_heat=2, scale=0.15, n_steps=5)
+    setups[1]["physical_parameters"] = dict(setups[1]["physical_parameters"], dynamic_viscosity=2e-3)
+    setups[4]["space_schemes"] = dict(setups[4]["space_schemes"], reconstructor=reconstructors.muscl)
+    k, out = _advance_pair(setups, 5)
+    assert k >= 3
+    for i, (a, b, ta, tb, st) in enumerate(out):
+        assert st == 0 and ta[1] == 5
+        assert rel_l2(a, b) <= 1e-5, (i, rel_l2(a, b))
+        assert abs(ta[0] - tb[0]) <= 1e-6 * tb[0]
+
+
+def test_mixed_launch_one_kind():
+    """Mixed launches of navier_stokes grids only and of heat grids only."""
+    from multiphysics_fvm_b200.setups import batch_mixed
+    for n_kh, n_heat in ((4, 0), (0, 3)):
+        setups = batch_mixed.make_setups(seed=6, n_kh=n_kh, n_heat=n_heat, scale=0.2, n_steps=4)
+        k, out = _advance_pair(setups, 4)
+        assert k == 1
+        for i, (a, b, ta, tb, st) in enumerate(out):
+            assert st == 0 and ta[1] == 4
+            assert rel_l2(a, b) <= 1e-5, (n_kh, n_heat, i, rel_l2(a, b))
 
 
 def test_autotune_restores_state():
