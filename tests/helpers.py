@@ -60,3 +60,30 @@ def random_ns_state(shape, rng, gam=1.4):
 
 def to_fp32(U):
     return U.astype(np.float32).astype(np.float64)
+
+
+KIND_NAMES = {0: "periodic", 1: "neumann", 2: "reflecting", 3: "dirichlet"}
+
+
+def setup_state(s):
+    """The setup's initial state as one [var, ...] array (ghosts included)."""
+    from multiphysics_fvm_b200.backend import VARIABLES, physics_name
+    from multiphysics_fvm_b200.grid.geometry import build_grid
+    g = build_grid(s["coordinate_system"], s["grid_config"])
+    U = s["physics"].allocate_u(s["grid_config"])
+    s["initial_conditions"]["initializer"](U, s["physical_parameters"], g, s["initial_conditions"]["parameters"])
+    return np.stack([U[k] for k in VARIABLES[physics_name(s["physics"])]])
+
+
+def oracle_bcs_of_setup(s):
+    """The setup's per-variable, per-side selectors as oracle (kind, value) pairs."""
+    from multiphysics_fvm_b200.backend import bc_codes, physics_name
+    rows = bc_codes(physics_name(s["physics"]), s["boundary_conditions"])
+    return [{side: (KIND_NAMES[k], v) for side, (k, v) in zip(O.SIDES, row)} for row in rows]
+
+
+def oracle_schemes_of_setup(s):
+    ss = s["space_schemes"]
+    name = lambda f: None if f is None else f.__name__  # noqa: E731
+    return dict(reconstructor=name(ss["reconstructor"]), slope_limiter=name(ss.get("slope_limiter")),
+                riemann_solver=name(ss.get("riemann_solver")))

@@ -117,3 +117,34 @@ def test_autotune_restores_state():
         got = b[i].download()[:, 1:-1, 1:-1, 1:-1]
         assert np.array_equal(got, U.astype(np.float32).astype(np.float64)[:, 1:-1, 1:-1, 1:-1])
     b.close()
+
+
+def test_batch_members_against_oracle():
+    """Three members of a mixed batch (two 2-D Kelvin-Helmholtz grids and one
+    cylindrical heat grid) against the oracle run of each setup from the same
+    float32-rounded state: relative L2 <= 1e-5 after 3 steps, time to 1e-5."""
+    import math
+    from multiphysics_fvm_b200.backend import Batch, physics_name
+    from multiphysics_fvm_b200.setups import batch_mixed
+    from oracle import fvm_oracle as O
+    from tests.helpers import oracle_bcs_of_setup, oracle_schemes_of_setup, setup_state, to_fp32
+    setups = batch_mixed.make_setups(seed=7, n_kh=2, n_heat=1, scale=0.25, n_steps=3)
+    states = [to_fp32(setup_state(s)) for s in setups]
+    b = Batch(setups)
+    assert b.launches_per_stage() == 1
+    for i, U in enumerate(states):
+        b[i].upload(U)
+        b[i].set_time(0.0, math.inf, float(setups[i]["time_config"]["CFL"]))
+    b.step(3)
+    I3 = (slice(None),) + (slice(1, -1),) * 3
+    for i, (s, U) in enumerate(zip(setups, states)):
+        Uo = U.copy()
+        dts = O.run(physics_name(s["physics"]), Uo, s["physical_parameters"],
+                    O.Geometry(s["coordinate_system"], s["grid_config"]), oracle_schemes_of_setup(s),
+                    oracle_bcs_of_setup(s), s["time_integrator"].__name__, float(s["time_config"]["CFL"]), 3)
+        t, steps, _ = b[i].time()
+        assert b[i].status() == 0 and steps == 3
+        assert abs(t - sum(dts)) <= 1e-5 * sum(dts), (i, t, sum(dts))
+        e = rel_l2(b[i].download()[I3], Uo[I3])
+        assert e <= 1e-5, (i, physics_name(s["physics"]), e)
+    b.close()

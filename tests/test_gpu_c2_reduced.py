@@ -27,43 +27,18 @@ import numpy as np
 import pytest
 
 from oracle import fvm_oracle as O
-from tests.helpers import bcs_dict, oracle_bcs, random_ns_state, rel_l2, rel_linf, to_fp32
+from tests.helpers import (bcs_dict, oracle_bcs, oracle_bcs_of_setup, oracle_schemes_of_setup, random_ns_state,
+                           rel_l2, rel_linf, setup_state, to_fp32)
 
 pytestmark = pytest.mark.gpu
 
 I3 = (slice(None),) + (slice(1, -1),) * 3
-KIND_NAMES = {0: "periodic", 1: "neumann", 2: "reflecting", 3: "dirichlet"}
-
-
-def _setup_state(s):
-    from multiphysics_fvm_b200.backend import VARIABLES, physics_name
-    from multiphysics_fvm_b200.grid.geometry import build_grid
-    g = build_grid(s["coordinate_system"], s["grid_config"])
-    U = s["physics"].allocate_u(s["grid_config"])
-    s["initial_conditions"]["initializer"](U, s["physical_parameters"], g, s["initial_conditions"]["parameters"])
-    return np.stack([U[k] for k in VARIABLES[physics_name(s["physics"])]])
-
-
-def _oracle_bcs_of_setup(s):
-    """The setup's per-variable, per-side selectors as oracle (kind, value) pairs."""
-    from multiphysics_fvm_b200.backend import bc_codes, physics_name
-    rows = bc_codes(physics_name(s["physics"]), s["boundary_conditions"])
-    return [{side: (KIND_NAMES[k], v) for side, (k, v) in zip(O.SIDES, row)} for row in rows]
-
-
-def _oracle_schemes_of_setup(s):
-    ss = s["space_schemes"]
-    name = lambda f: None if f is None else f.__name__  # noqa: E731
-    return dict(reconstructor=name(ss["reconstructor"]), slope_limiter=name(ss.get("slope_limiter")),
-                riemann_solver=name(ss.get("riemann_solver")))
-
-
 def _run_setup_against_oracle(s, physics, integrator, n_steps):
     from multiphysics_fvm_b200.backend import Simulation
-    U0 = _setup_state(s)
+    U0 = setup_state(s)
     geo = O.Geometry(s["coordinate_system"], s["grid_config"])
-    sch = _oracle_schemes_of_setup(s)
-    bcs = _oracle_bcs_of_setup(s)
+    sch = oracle_schemes_of_setup(s)
+    bcs = oracle_bcs_of_setup(s)
     cfl = float(s["time_config"]["CFL"])
     results = {}
     for precision, tol, ttol in (("fp64", 1e-10, 1e-12), ("fp32", 1e-4, 1e-5)):
