@@ -69,6 +69,43 @@ struct Layout {
   }
 };
 
+// Boundary selector of every variable and side (boundary_conditions.py:13-91
+// applied per variable and side as in solver.py:30-37).
+struct BcSpec {
+  signed char kind[6][6];  // [var][side]: 0 periodic, 1 neumann, 2 reflecting, 3 dirichlet
+  double value[6][6];
+};
+
+// Ghost faces written by the stage that produces the interior: a cell that is
+// the source of a ghost face cell (the adjacent layer, or for periodic sides
+// the opposite layer) stores that ghost too, with the value the separate fill
+// (bc_fill_kernel) would give: v, -v (reflecting) or 2w - v (Dirichlet w).
+// (i, j, k) are the ghosted indices of an interior cell, v its new value of
+// variable q.  Faces only: edges and corners are never read.
+__host__ __device__ inline bool on_boundary_layer(const Layout& L, int i, int j, int k) {
+  return i == 1 || i == L.nx || j == 1 || j == L.ny || k == 1 || k == L.nz;
+}
+template <typename Real>
+__device__ __forceinline__ void store_ghosts(Real* __restrict__ out, const Layout& L, const BcSpec& bc, int q, int i,
+                                             int j, int k, Real v) {
+  const int n[3] = {L.nx, L.ny, L.nz};
+  const int c[3] = {i, j, k};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+#pragma unroll
+    for (int hi = 0; hi < 2; ++hi) {
+      const int kind = bc.kind[q][2 * a + hi];
+      const int src = kind == 0 ? (hi ? 1 : n[a]) : (hi ? n[a] : 1);
+      if (c[a] == src) {
+        int g[3] = {i, j, k};
+        g[a] = hi ? n[a] + 1 : 0;
+        const Real w2 = Real(2) * Real(bc.value[q][2 * a + hi]);
+        out[L.idx(q, g[2], g[1], g[0])] = kind == 2 ? -v : (kind == 3 ? w2 - v : v);
+      }
+    }
+  }
+}
+
 // Cell metrics (interior cell i,j,k, 0-based).  Products keep the reference's
 // left-to-right order so that the float64 build reproduces NumPy bitwise.
 template <typename Real, int COORD>

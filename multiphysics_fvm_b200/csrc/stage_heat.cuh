@@ -29,6 +29,7 @@ struct HeatParams {
   unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
   unsigned long long drain_ns;  // limit of the wait for copies in flight after a timeout (ns)
   unsigned extra_tx;  // test of the timeout path: bytes a ring copy never delivers (0 normally)
+  const BcSpec* ghosts;  // non-null: the stage also writes the ghost faces of `out`
 };
 
 template <typename Real, int LIM, int TY>
@@ -230,6 +231,7 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
           const Real u0v = (needs_u0<Real>(p.coef) && p.coef.u0_is_input) ? ucur : eu0, accv = eacc;
           const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
           p.out[gi] = o;
+          if (p.ghosts && on_boundary_layer(L, oi + 1, oj + 1, K)) store_ghosts(p.out, L, *p.ghosts, 0, oi + 1, oj + 1, K, o);
           if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
           if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
         }
@@ -296,6 +298,7 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         const Real u0v = (needs_u0<Real>(p.coef) && p.coef.u0_is_input) ? ucur : eu0, accv = eacc;
         const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
         p.out[gi] = o;
+        if (p.ghosts && on_boundary_layer(L, oi + 1, oj + 1, K)) store_ghosts(p.out, L, *p.ghosts, 0, oi + 1, oj + 1, K, o);
         if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
         if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
       }

@@ -157,6 +157,7 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
           ph2[t] = g2[t] * (uK[o + W] - uK[o - W]);
         }
         unsigned bad = 0;
+        float ov[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int o = (w * R + r + HH) * W + lane + 4;
@@ -173,11 +174,18 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
             const float u0v = need_u0 ? eu0[r] : u0c;
             const float o2 = stage_combine(p.coef, dt, k, u0c, u0v, eacc[r]);
             p.out[gi] = o2;
+            ov[r] = o2;
             if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, eacc[r]);
             if (!isfinite(o2)) bad |= ST_NONFINITE;
           }
         }
         if (bad) atomicOr(p.status, bad);
+        // ghost faces copied from this strip's boundary cells
+        if (p.ghosts && icol && (i == 0 || i == nx - 1 || jb == 0 || jb + R >= ny || K == 1 || K == nz)) {
+#pragma unroll
+          for (int r = 0; r < R; ++r)
+            if (jb + r < ny) store_ghosts(p.out, L, *p.ghosts, 0, i + 1, jb + r + 1, K, ov[r]);
+        }
       }
 #pragma unroll
       for (int r = 0; r < R; ++r) {

@@ -31,6 +31,7 @@ struct MaxwellParams {
   unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
   unsigned long long drain_ns;  // limit of the wait for copies in flight after a timeout (ns)
   unsigned extra_tx;  // test of the timeout path: bytes a ring copy never delivers (0 normally)
+  const BcSpec* ghosts;  // non-null: the stage also writes the ghost faces of `out`
 };
 
 template <typename Real, int TY>
@@ -445,11 +446,13 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
           }
         }
         unsigned bad = 0;
+        const bool gb = p.ghosts && on_boundary_layer(L, oi + 1, oj + 1, K);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const long long gi = gidx + (long long)v * L.var_stride;
           const Real o = stage_combine(p.coef, dt, kv[v], q[v], u0v[v], accv[v]);
           p.out[gi] = o;
+          if (gb) store_ghosts(p.out, L, *p.ghosts, v, oi + 1, oj + 1, K, o);
           if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, kv[v], u0v[v], accv[v]);
           if (!isfinite(o)) bad |= ST_NONFINITE;
         }

@@ -470,6 +470,7 @@ __global__ void __launch_bounds__(MxStripCfg<R, NW>::NT, MINB)
               }
               const long long g = L.idx(0, K, j + 1, i + 1);
               const int so = ty * TX + lane;
+              const bool gb = p.ghosts && on_boundary_layer(L, i + 1, j + 1, K);
 #pragma unroll
               for (int v = 0; v < NV; ++v) {
                 const float k = src_[v] - kv[r][v];
@@ -478,6 +479,7 @@ __global__ void __launch_bounds__(MxStripCfg<R, NW>::NT, MINB)
                 const long long gi = g + (long long)v * L.var_stride;
                 const float o2 = stage_combine(p.coef, dt, k, q[v], u0v, accv);
                 p.out[gi] = o2;
+                if (gb) store_ghosts(p.out, L, *p.ghosts, v, i + 1, j + 1, K, o2);
                 if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
                 if (!isfinite(o2)) bad |= ST_NONFINITE;
               }
