@@ -209,31 +209,54 @@ __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, co
   __shared__ double s_rc[32], s_nu[32];
   double rc = 0.0, nu = 0.0;
   unsigned bad = 0;
-  // x1 rows (rows = ny*nz < 2^31, no 64-bit division per cell), threads across
-  // the row.  Each thread first loads its cell of RB rows (RB*5 loads in
-  // flight) and then runs the float64 arithmetic, whose division and square
-  // root chains would otherwise leave the loads of one row exposed.
-  constexpr int RB = 4;
-  const int rows = L.ny * L.nz;
-  const int G = gridDim.x;
-  for (int row0 = blockIdx.x; row0 < rows; row0 += RB * G) {
-    for (int i = threadIdx.x; i < L.nx; i += blockDim.x) {
-      Real q[RB][5];
-      int jr[RB], kr[RB];
+  // Work items are 32-cell pieces of x1 rows, one per warp at a time, so narrow
+  // grids keep every lane busy.  A warp's items are nwarp apart in the order
+  // (piece, j, k); its cursor (c, j, k) advances by that stride with carries,
+  // without divisions.  A warp loads IB items ahead of the float64 arithmetic,
+  // whose division and square-root chains would otherwise leave the loads
+  // exposed.
+  constexpr int IB = 2;
+  const int nch = (L.nx + 31) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int nwarp = gridDim.x * (blockDim.x >> 5);
+  const int w0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int dq = nwarp / nch, dr = nwarp % nch, rj = dq % L.ny, rk = dq / L.ny;
+  int cc = w0 % nch, cj = (w0 / nch) % L.ny, ck = (w0 / nch) / L.ny;  // load cursor
+  auto advance = [&]() {
+    cc += dr;
+    cj += rj;
+    ck += rk;
+    if (cc >= nch) { cc -= nch; cj += 1; }
+    if (cj >= L.ny) { cj -= L.ny; ck += 1; }
+  };
+  auto load = [&](Real* q, int* ijk) {
+    const int i = cc * 32 + lane;
+    const bool in = ck < L.nz && i < L.nx;
+    ijk[0] = in ? i : -1;
+    ijk[1] = cj;
+    ijk[2] = ck;
+    const long long g = in ? L.idx(0, ck + 1, cj + 1, i + 1) : 0;
 #pragma unroll
-      for (int b = 0; b < RB; ++b) {
-        const int row = row0 + b * G;
-        const bool in = row < rows;
-        jr[b] = in ? row % L.ny : 0;
-        kr[b] = in ? row / L.ny : 0;
-        const long long g = L.idx(0, kr[b] + 1, jr[b] + 1, 1) + i;
+    for (int v = 0; v < 5; ++v) q[v] = in ? u[g + v * L.var_stride] : Real(1);
+    advance();
+  };
+  Real q[IB][5];
+  int at[IB][3];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) q[b][v] = in ? u[g + v * L.var_stride] : Real(1);
-      }
+  for (int b = 0; b < IB; ++b) load(q[b], at[b]);
+  for (;;) {
+    bool any = false;
 #pragma unroll
-      for (int b = 0; b < RB; ++b) {
-        if (row0 + b * G >= rows) continue;
-        const int j = jr[b], k = kr[b];
+    for (int b = 0; b < IB; ++b) any |= at[b][2] < L.nz;
+    if (!any) break;  // warp-uniform: every lane's cursor has left the grid
+    Real qn[IB][5];
+    int an[IB][3];
+#pragma unroll
+    for (int b = 0; b < IB; ++b) load(qn[b], an[b]);
+#pragma unroll
+    for (int b = 0; b < IB; ++b) {
+      if (at[b][0] >= 0) {
+        const int i = at[b][0], j = at[b][1], k = at[b][2];
         // float64 throughout; one reciprocal of rho and the inverse-length
         // tables replace the eight divisions (dt moves by ulps, inside 1e-12)
         const double rho = double(q[b][0]);
@@ -255,6 +278,13 @@ __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, co
         rc = fmax(rc, r);
         nu = fmax(nu, nl);
       }
+    }
+#pragma unroll
+    for (int b = 0; b < IB; ++b) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) at[b][c] = an[b][c];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) q[b][v] = qn[b][v];
     }
   }
   for (int o = 16; o > 0; o >>= 1) {

@@ -76,34 +76,37 @@ struct BcSpec {
   double value[6][6];
 };
 
-// Ghost faces written by the stage that produces the interior: a cell that is
-// the source of a ghost face cell (the adjacent layer, or for periodic sides
-// the opposite layer) stores that ghost too, with the value the separate fill
-// (bc_fill_kernel) would give: v, -v (reflecting) or 2w - v (Dirichlet w).
-// (i, j, k) are the ghosted indices of an interior cell, v its new value of
-// variable q.  Faces only: edges and corners are never read.
-__host__ __device__ inline bool on_boundary_layer(const Layout& L, int i, int j, int k) {
-  return i == 1 || i == L.nx || j == 1 || j == L.ny || k == 1 || k == L.nz;
-}
+// Ghost faces written by the stage that produces the interior, one tile at a
+// time: after a block has stored a tile's cells (0-based x1 in [xa, xb), x2 in
+// [ya, yb), ghosted planes za..zb) and passed a block barrier, it copies those
+// that are the source of a ghost face cell (the adjacent layer, or for a
+// periodic side the opposite layer) into the ghost, with the value the
+// separate fill (bc_fill_kernel) gives: v, -v (reflecting) or 2w - v
+// (Dirichlet w).  Faces only: edges and corners are never read.  Tiles away
+// from the domain boundary have nothing to do.
 template <typename Real>
-__device__ __forceinline__ void store_ghosts(Real* __restrict__ out, const Layout& L, const BcSpec& bc, int q, int i,
-                                             int j, int k, Real v) {
+__device__ __noinline__ void tile_ghosts(Real* out, const Layout& L, const BcSpec& bc, int nv, int xa, int xb,
+                                         int ya, int yb, int za, int zb) {
+  const int tid = threadIdx.x, nt = blockDim.x;
   const int n[3] = {L.nx, L.ny, L.nz};
-  const int c[3] = {i, j, k};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-#pragma unroll
-    for (int hi = 0; hi < 2; ++hi) {
-      const int kind = bc.kind[q][2 * a + hi];
-      const int src = kind == 0 ? (hi ? 1 : n[a]) : (hi ? n[a] : 1);
-      if (c[a] == src) {
-        int g[3] = {i, j, k};
-        g[a] = hi ? n[a] + 1 : 0;
-        const Real w2 = Real(2) * Real(bc.value[q][2 * a + hi]);
-        out[L.idx(q, g[2], g[1], g[0])] = kind == 2 ? -v : (kind == 3 ? w2 - v : v);
+  for (int q = 0; q < nv; ++q)
+    for (int s = 0; s < 6; ++s) {
+      const int a = s >> 1, hi = s & 1;
+      const int kind = bc.kind[q][s];
+      const int src = kind == 0 ? (hi ? 1 : n[a]) : (hi ? n[a] : 1);  // ghosted index of the source layer
+      int lo[3] = {xa + 1, ya + 1, za}, up[3] = {xb, yb, zb};
+      if (src < lo[a] || src > up[a]) continue;
+      lo[a] = up[a] = src;
+      const int e0 = up[0] - lo[0] + 1, e1 = up[1] - lo[1] + 1, e2 = up[2] - lo[2] + 1;
+      const int cnt = e0 * e1 * e2;
+      const Real w2 = Real(2) * Real(bc.value[q][s]);
+      for (int t = tid; t < cnt; t += nt) {
+        int c[3] = {lo[0] + t % e0, lo[1] + (t / e0) % e1, lo[2] + t / (e0 * e1)};
+        const Real v = out[L.idx(q, c[2], c[1], c[0])];
+        c[a] = hi ? n[a] + 1 : 0;
+        out[L.idx(q, c[2], c[1], c[0])] = kind == 2 ? -v : (kind == 3 ? w2 - v : v);
       }
     }
-  }
 }
 
 // Cell metrics (interior cell i,j,k, 0-based).  Products keep the reference's

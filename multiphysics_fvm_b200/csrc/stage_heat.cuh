@@ -231,7 +231,6 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
           const Real u0v = (needs_u0<Real>(p.coef) && p.coef.u0_is_input) ? ucur : eu0, accv = eacc;
           const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
           p.out[gi] = o;
-          if (p.ghosts && on_boundary_layer(L, oi + 1, oj + 1, K)) store_ghosts(p.out, L, *p.ghosts, 0, oi + 1, oj + 1, K, o);
           if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
           if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
         }
@@ -298,12 +297,12 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
         const Real u0v = (needs_u0<Real>(p.coef) && p.coef.u0_is_input) ? ucur : eu0, accv = eacc;
         const Real o = stage_combine(p.coef, dt, k, ucur, u0v, accv);
         p.out[gi] = o;
-        if (p.ghosts && on_boundary_layer(L, oi + 1, oj + 1, K)) store_ghosts(p.out, L, *p.ghosts, 0, oi + 1, oj + 1, K, o);
         if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
         if (!isfinite(o)) atomicOr(p.status, ST_NONFINITE);
       }
     }
     __syncthreads();  // the next tile's first loads reuse every ring slot
+    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, 1, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   if (!ok && tid == 0)
     for (int s = 0; s < C::NSLOT; ++s)

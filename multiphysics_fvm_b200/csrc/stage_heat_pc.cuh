@@ -157,7 +157,6 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
           ph2[t] = g2[t] * (uK[o + W] - uK[o - W]);
         }
         unsigned bad = 0;
-        float ov[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int o = (w * R + r + HH) * W + lane + 4;
@@ -174,18 +173,11 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
             const float u0v = need_u0 ? eu0[r] : u0c;
             const float o2 = stage_combine(p.coef, dt, k, u0c, u0v, eacc[r]);
             p.out[gi] = o2;
-            ov[r] = o2;
             if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, eacc[r]);
             if (!isfinite(o2)) bad |= ST_NONFINITE;
           }
         }
         if (bad) atomicOr(p.status, bad);
-        // ghost faces copied from this strip's boundary cells
-        if (p.ghosts && icol && (i == 0 || i == nx - 1 || jb == 0 || jb + R >= ny || K == 1 || K == nz)) {
-#pragma unroll
-          for (int r = 0; r < R; ++r)
-            if (jb + r < ny) store_ghosts(p.out, L, *p.ghosts, 0, i + 1, jb + r + 1, K, ov[r]);
-        }
       }
 #pragma unroll
       for (int r = 0; r < R; ++r) {
@@ -194,12 +186,14 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
       }
       __syncthreads();  // plane K's slot is refilled at the next step
     }
+    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, 1, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   return true;
 }
 
+// 768 resident threads per SM (6 blocks of 4 warps): at most 80 registers.
 template <int COORD, int R, int NW>
-__global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT)
+__global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT, 768 / HeatPcCfg<R, NW>::NT)
     heat_pc_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ HeatParams<float> p) {
   using C = HeatPcCfg<R, NW>;
   extern __shared__ __align__(128) unsigned char smem_raw[];

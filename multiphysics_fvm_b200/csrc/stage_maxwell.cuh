@@ -446,13 +446,11 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
           }
         }
         unsigned bad = 0;
-        const bool gb = p.ghosts && on_boundary_layer(L, oi + 1, oj + 1, K);
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const long long gi = gidx + (long long)v * L.var_stride;
           const Real o = stage_combine(p.coef, dt, kv[v], q[v], u0v[v], accv[v]);
           p.out[gi] = o;
-          if (gb) store_ghosts(p.out, L, *p.ghosts, v, oi + 1, oj + 1, K, o);
           if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, kv[v], u0v[v], accv[v]);
           if (!isfinite(o)) bad |= ST_NONFINITE;
         }
@@ -460,6 +458,7 @@ __global__ void __launch_bounds__(MaxwellCfg<Real, TY>::NT, MINB)
       }
     }
     __syncthreads();  // the next tile's first loads reuse every ring slot
+    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, NV, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   if constexpr (STAGED) cp_async_wait_all();  // none left in flight at exit
   if (!ok && tid == 0)

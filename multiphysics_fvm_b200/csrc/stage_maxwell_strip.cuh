@@ -470,7 +470,6 @@ __global__ void __launch_bounds__(MxStripCfg<R, NW>::NT, MINB)
               }
               const long long g = L.idx(0, K, j + 1, i + 1);
               const int so = ty * TX + lane;
-              const bool gb = p.ghosts && on_boundary_layer(L, i + 1, j + 1, K);
 #pragma unroll
               for (int v = 0; v < NV; ++v) {
                 const float k = src_[v] - kv[r][v];
@@ -479,7 +478,6 @@ __global__ void __launch_bounds__(MxStripCfg<R, NW>::NT, MINB)
                 const long long gi = g + (long long)v * L.var_stride;
                 const float o2 = stage_combine(p.coef, dt, k, q[v], u0v, accv);
                 p.out[gi] = o2;
-                if (gb) store_ghosts(p.out, L, *p.ghosts, v, i + 1, j + 1, K, o2);
                 if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
                 if (!isfinite(o2)) bad |= ST_NONFINITE;
               }
@@ -512,6 +510,8 @@ __global__ void __launch_bounds__(MxStripCfg<R, NW>::NT, MINB)
         break;
       }
     }
+    if (!ok) break;
+    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, NV, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   if (!ok && tid == 0) {
     for (int s = 0; s < C::NBAR; ++s)

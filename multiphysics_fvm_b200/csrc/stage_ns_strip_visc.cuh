@@ -526,7 +526,6 @@ __global__ void __launch_bounds__(NsStripViscCfg<R, NW>::NT, MINB)
               const float sg[5] = {0.f, q[0] * gx, q[0] * gy, q[0] * gz, fmaf(gx, q[1], fmaf(gy, q[2], gz * q[3]))};
               const long long g = L.idx(0, K, j + 1, i + 1);
               const int so = ty * TX + lane;
-              const bool gb = p.ghosts && on_boundary_layer(L, i + 1, j + 1, K);
 #pragma unroll
               for (int v = 0; v < 5; ++v) {
                 const float k = sg[v] - kv[r][v];
@@ -535,7 +534,6 @@ __global__ void __launch_bounds__(NsStripViscCfg<R, NW>::NT, MINB)
                 const long long gi = g + (long long)v * L.var_stride;
                 const float o2 = stage_combine(p.coef, dt, k, q[v], u0v, accv);
                 p.out[gi] = o2;
-                if (gb) store_ghosts(p.out, L, *p.ghosts, v, i + 1, j + 1, K, o2);
                 if (p.coef.accmode != ACC_NONE) p.acc[gi] = acc_update(p.coef, dt, k, u0v, accv);
                 if (!isfinite(o2)) bad |= ST_NONFINITE;
                 if (v == 0 && p.coef.mode != MODE_RHS && !(o2 > 0.f)) bad |= ST_DENSITY;
@@ -550,6 +548,8 @@ __global__ void __launch_bounds__(NsStripViscCfg<R, NW>::NT, MINB)
         break;
       }
     }
+    if (!ok) break;
+    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, 5, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   if (!ok && tid == 0) {
     for (int s = 0; s < C::NBAR; ++s)

@@ -71,6 +71,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--precision", default=None)
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--tile-rows", type=int, default=0, help="block shape (tile rows); 0: the default")
+    ap.add_argument("--zchunk", type=int, default=0, help="z-march depth (planes per tile); 0: the default")
     ap.add_argument("--breakdown", action="store_true",
                     help="also time each launch of a few un-captured steps: stage kernels vs the rest")
     a = ap.parse_args()
@@ -78,7 +80,7 @@ def main():
         run_batch(a.steps, a.warmup, a.autotune)
         return
     s, U = make(a.config, a.n, a.precision)
-    sim = backend.Simulation.from_setup(s)
+    sim = backend.Simulation.from_setup(s, tile_ty=a.tile_rows, zchunk=a.zchunk)
     sim.upload(U)
     sim.set_time(0.0, math.inf, float(s["time_config"]["CFL"]))
     tuned = sim.autotune() if a.autotune else None
