@@ -101,7 +101,6 @@ struct fvm_handle {
   cudaStream_t stream = nullptr;
   void* U[3] = {nullptr, nullptr, nullptr};  // base, stage a, stage b
   void* acc = nullptr;
-  BcSpec* bc_dev = nullptr;     // boundary selectors for the stage kernels' ghost-face stores
   void* met_real = nullptr;     // metric tables in the state precision
   double* met_f64 = nullptr;    // metric tables in float64 (reductions)
   Metric<float> mf{};
@@ -360,9 +359,6 @@ void fill_common(fvm_handle* h, const StageDef& sd, bool rhs_only, P& p) {
   p.wait_ns = h->wait_ns;
   p.drain_ns = h->drain_ns;
   p.extra_tx = h->extra_tx;
-  // stage outputs carry their ghost faces, except under the closure, whose
-  // correction changes the interior after the stage (a separate fill follows it)
-  p.ghosts = (!rhs_only && !h->closure) ? h->bc_dev : nullptr;
 }
 
 // x3 fluxes cancel exactly on a one-plane grid whose x3 ghosts copy the plane
@@ -536,13 +532,8 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
                                            (float)h->d.params[0], h->stream);
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("closure: ") + cudaGetErrorString(e));
   }
-  // Ghost faces: the step's base state is filled here (it may come from an
-  // upload, whose ghosts the residual uses as given); every later stage input
-  // got its ghost faces from the stage kernel that wrote it.
-  bool first = true;
   for (const StageDef& sd : stage_table(h->d.integrator)) {
-    cudaError_t e = (first || h->closure) ? launch_bc(h, sd.in, true) : cudaSuccess;
-    first = false;
+    cudaError_t e = launch_bc(h, sd.in, true);
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
     if ((rc = close(false))) return rc;
     if ((rc = mark(pf ? pf->a : nullptr))) return rc;
@@ -685,11 +676,6 @@ int fvm_create(const fvm_desc* desc, fvm_handle** out) {
   FVM_CKC(cudaMemcpy(h->clk, &c0, sizeof(Clock), cudaMemcpyHostToDevice));
   FVM_CKC(cudaMalloc(&h->status, sizeof(unsigned)));
   FVM_CKC(cudaMemset(h->status, 0, sizeof(unsigned)));
-  {
-    const BcSpec bc = make_bc(h->d, h->nv);
-    FVM_CKC(cudaMalloc(&h->bc_dev, sizeof(BcSpec)));
-    FVM_CKC(cudaMemcpy(h->bc_dev, &bc, sizeof(BcSpec), cudaMemcpyHostToDevice));
-  }
   FVM_CKC(cudaMalloc(&h->partials, sizeof(double) * 8 * 1024));
   FVM_CKC(cudaMalloc(&h->totals_dev, sizeof(double) * 8));
   h->stage_elems = (size_t)h->nv * (d.nx1 + 2) * (d.nx2 + 2) * (d.nx3 + 2);
@@ -722,7 +708,6 @@ int fvm_destroy(fvm_handle* h) {
   if (h->met_real && h->met_real != h->met_f64) cudaFree(h->met_real);
   if (h->met_f64) cudaFree(h->met_f64);
   if (h->clk) cudaFree(h->clk);
-  if (h->bc_dev) cudaFree(h->bc_dev);
   if (h->status) cudaFree(h->status);
   if (h->partials) cudaFree(h->partials);
   if (h->totals_dev) cudaFree(h->totals_dev);
@@ -1325,12 +1310,9 @@ int enqueue_batch_step(fvm_batch* b, int dt_mode) {
   const std::vector<StageDef> st = stage_table(b->integrator);
   const int bcb = (int)std::min<long long>((b->faces + 255) / 256, 8192);
   for (size_t si = 0; si < st.size(); ++si) {
-    // the base state's ghost faces; later stage inputs got theirs from the stage kernels
-    if (si == 0) {
-      if (b->f64) batch_bc_kernel<double><<<bcb, 256, 0, b->stream>>>(b->aux, n, b->faces, st[si].in);
-      else batch_bc_kernel<float><<<bcb, 256, 0, b->stream>>>(b->aux, n, b->faces, st[si].in);
-      FVM_CK(cudaGetLastError());
-    }
+    if (b->f64) batch_bc_kernel<double><<<bcb, 256, 0, b->stream>>>(b->aux, n, b->faces, st[si].in);
+    else batch_bc_kernel<float><<<bcb, 256, 0, b->stream>>>(b->aux, n, b->faces, st[si].in);
+    FVM_CK(cudaGetLastError());
     for (auto& g : b->groups) {
       cudaError_t e = b->f64 ? launch_group_stage<double>(b, g, (int)si, b->nsm)
                              : launch_group_stage<float>(b, g, (int)si, b->nsm);

@@ -4,6 +4,11 @@
 
 namespace fvm {
 
+struct BcSpec {
+  signed char kind[6][6];  // [var][side]: 0 periodic, 1 neumann, 2 reflecting, 3 dirichlet
+  double value[6][6];
+};
+
 // Ghost face slabs of every variable (boundary_conditions.py:13-91 applied
 // per variable and side as in solver.py:30-37).  Edges and corners are never
 // read by the residual, so only the six face slabs are filled here.

@@ -69,46 +69,6 @@ struct Layout {
   }
 };
 
-// Boundary selector of every variable and side (boundary_conditions.py:13-91
-// applied per variable and side as in solver.py:30-37).
-struct BcSpec {
-  signed char kind[6][6];  // [var][side]: 0 periodic, 1 neumann, 2 reflecting, 3 dirichlet
-  double value[6][6];
-};
-
-// Ghost faces written by the stage that produces the interior, one tile at a
-// time: after a block has stored a tile's cells (0-based x1 in [xa, xb), x2 in
-// [ya, yb), ghosted planes za..zb) and passed a block barrier, it copies those
-// that are the source of a ghost face cell (the adjacent layer, or for a
-// periodic side the opposite layer) into the ghost, with the value the
-// separate fill (bc_fill_kernel) gives: v, -v (reflecting) or 2w - v
-// (Dirichlet w).  Faces only: edges and corners are never read.  Tiles away
-// from the domain boundary have nothing to do.
-template <typename Real>
-__device__ __noinline__ void tile_ghosts(Real* out, const Layout& L, const BcSpec& bc, int nv, int xa, int xb,
-                                         int ya, int yb, int za, int zb) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int n[3] = {L.nx, L.ny, L.nz};
-  for (int q = 0; q < nv; ++q)
-    for (int s = 0; s < 6; ++s) {
-      const int a = s >> 1, hi = s & 1;
-      const int kind = bc.kind[q][s];
-      const int src = kind == 0 ? (hi ? 1 : n[a]) : (hi ? n[a] : 1);  // ghosted index of the source layer
-      int lo[3] = {xa + 1, ya + 1, za}, up[3] = {xb, yb, zb};
-      if (src < lo[a] || src > up[a]) continue;
-      lo[a] = up[a] = src;
-      const int e0 = up[0] - lo[0] + 1, e1 = up[1] - lo[1] + 1, e2 = up[2] - lo[2] + 1;
-      const int cnt = e0 * e1 * e2;
-      const Real w2 = Real(2) * Real(bc.value[q][s]);
-      for (int t = tid; t < cnt; t += nt) {
-        int c[3] = {lo[0] + t % e0, lo[1] + (t / e0) % e1, lo[2] + t / (e0 * e1)};
-        const Real v = out[L.idx(q, c[2], c[1], c[0])];
-        c[a] = hi ? n[a] + 1 : 0;
-        out[L.idx(q, c[2], c[1], c[0])] = kind == 2 ? -v : (kind == 3 ? w2 - v : v);
-      }
-    }
-}
-
 // Cell metrics (interior cell i,j,k, 0-based).  Products keep the reference's
 // left-to-right order so that the float64 build reproduces NumPy bitwise.
 template <typename Real, int COORD>

@@ -29,7 +29,6 @@ struct HeatParams {
   unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
   unsigned long long drain_ns;  // limit of the wait for copies in flight after a timeout (ns)
   unsigned extra_tx;  // test of the timeout path: bytes a ring copy never delivers (0 normally)
-  const BcSpec* ghosts;  // non-null: the stage also writes the ghost faces of `out`
 };
 
 template <typename Real, int LIM, int TY>
@@ -302,7 +301,6 @@ __global__ void __launch_bounds__(HeatCfg<Real, LIM, TY>::NT, 1)
       }
     }
     __syncthreads();  // the next tile's first loads reuse every ring slot
-    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, 1, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   if (!ok && tid == 0)
     for (int s = 0; s < C::NSLOT; ++s)

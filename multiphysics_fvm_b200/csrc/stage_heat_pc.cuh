@@ -186,14 +186,12 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
       }
       __syncthreads();  // plane K's slot is refilled at the next step
     }
-    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, 1, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   return true;
 }
 
-// 768 resident threads per SM (6 blocks of 4 warps): at most 80 registers.
 template <int COORD, int R, int NW>
-__global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT, 768 / HeatPcCfg<R, NW>::NT)
+__global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT)
     heat_pc_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ HeatParams<float> p) {
   using C = HeatPcCfg<R, NW>;
   extern __shared__ __align__(128) unsigned char smem_raw[];

@@ -37,7 +37,6 @@ struct NsParams {
   unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
   unsigned long long drain_ns;  // limit of the wait for copies in flight after a timeout (ns)
   unsigned extra_tx;  // test of the timeout path: bytes a ring copy never delivers (0 normally)
-  const BcSpec* ghosts;  // non-null: the stage also writes the ghost faces of `out`
 };
 
 // Tile sources: one grid (params + tensor map in kernel parameter space) or a
@@ -743,7 +742,6 @@ __global__ void __launch_bounds__(NsCfg<Real, VISC, TY>::NT, MINB)
       }
     }
     __syncthreads();  // the next tile's first loads reuse every ring slot
-    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, 5, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   if constexpr (STAGED) cp_async_wait_all();  // none left in flight at exit
   // On a timeout, wait (bounded) for every load this block may still have in flight.

@@ -511,7 +511,6 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
       // ------------------------------------------------------------ 7 ----
       if (!__syncthreads_and(step_ok)) return false;
     }
-    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, 5, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   return true;
 }

@@ -548,8 +548,6 @@ __global__ void __launch_bounds__(NsStripViscCfg<R, NW>::NT, MINB)
         break;
       }
     }
-    if (!ok) break;
-    if (p.ghosts) tile_ghosts(p.out, L, *p.ghosts, 5, x0, min(x0 + TX, nx), y0, min(y0 + TY, ny), Z0, Zl);
   }
   if (!ok && tid == 0) {
     for (int s = 0; s < C::NBAR; ++s)
