@@ -340,7 +340,9 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (each state buffer 345 MB > 126 MB)",
                        "timing": "CUDA events on the handle stream around K graph launches, max over ranks",
                        "zchunk": zchunk},
-            "gpu_launches": args.steps * (2 + 2 * len(STAGE_BYTES)),
+            # per step: the CFL reduction, then per stage a ghost fill (the first one
+            # also closes the clock) and the stage kernel
+            "gpu_launches": args.steps * (1 + 2 * len(STAGE_BYTES)),
             "device_status": status,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_source,

@@ -455,13 +455,18 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
                          make_ns_params<Real>(h, sd, rhs_only), h->stream, nsm, h->tile_ty);
 }
 
-cudaError_t launch_bc(fvm_handle* h, int b, bool use_active) {
+// Ghost fill of state buffer b; `ck` (optional) also closes the step's clock.
+cudaError_t launch_bc(fvm_handle* h, int b, const ClockArgs* ck = nullptr) {
   const Layout& L = h->lay;
-  const dim3 grid((unsigned)std::min(std::max(L.nz, L.ny), 4096), (unsigned)(6 * h->nv));
+  const long long face = std::max({(long long)L.ny * L.nz, (long long)L.nx * L.nz, (long long)L.nx * L.ny});
+  // about one resident wave: blocks per face row up to 8 blocks/SM over all rows
+  const long long per_row = std::max(1LL, std::min((face + 256LL * BCF - 1) / (256LL * BCF),
+                                                   (8LL * h->nsm + 6 * h->nv - 1) / (6 * h->nv)));
+  const dim3 grid((unsigned)per_row, (unsigned)(6 * h->nv));
   const BcSpec bc = make_bc(h->d, h->nv);
-  const int* act = use_active ? &h->clk->active : nullptr;
-  if (h->f64) bc_fill_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<double*>(h->U[b]), L, h->nv, bc, act);
-  else bc_fill_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<float*>(h->U[b]), L, h->nv, bc, act);
+  const ClockArgs c = ck ? *ck : ClockArgs{nullptr, 0, 0.0, 0.0, nullptr};
+  if (h->f64) bc_fill_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<double*>(h->U[b]), L, h->nv, bc, c);
+  else bc_fill_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<float*>(h->U[b]), L, h->nv, bc, c);
   return cudaGetLastError();
 }
 
@@ -523,17 +528,24 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
     cudaError_t e = h->f64 ? launch_dt_reduce<double>(h) : launch_dt_reduce<float>(h);
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("dt reduction: ") + cudaGetErrorString(e));
   }
+  // the first stage's ghost fill also closes the clock (dt, t, step count, active)
   const int cmode = dt_mode == 1 ? 1 : (state_dt ? 0 : 2);
-  clock_kernel<<<1, 1, 0, h->stream>>>(h->clk, cmode, h->max_inv_l2, h->const_rate, h->status);
-  FVM_CK(cudaGetLastError());
+  const ClockArgs ck{h->clk, cmode, h->max_inv_l2, h->const_rate, h->status};
+  {
+    const StageDef& s0 = stage_table(h->d.integrator).front();
+    cudaError_t e = launch_bc(h, s0.in, &ck);
+    if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
+  }
   if (h->closure) {
     // face corrections from the step's base state (periodic: no ghosts read)
     cudaError_t e = closure::enqueue_infer(h->closure, static_cast<const float*>(h->U[0]), h->lay,
                                            (float)h->d.params[0], h->stream);
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("closure: ") + cudaGetErrorString(e));
   }
+  bool first = true;
   for (const StageDef& sd : stage_table(h->d.integrator)) {
-    cudaError_t e = launch_bc(h, sd.in, true);
+    cudaError_t e = first ? cudaSuccess : launch_bc(h, sd.in);
+    first = false;
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
     if ((rc = close(false))) return rc;
     if ((rc = mark(pf ? pf->a : nullptr))) return rc;
@@ -801,7 +813,7 @@ static void fill_edges_corners(double* f, int n1, int n2, int n3) {
 
 int fvm_download(fvm_handle* h, double* host_state) {
   if (!h || !host_state) return fail(FVM_E_INVALID, "null argument");
-  FVM_CK(launch_bc(h, 0, false));
+  FVM_CK(launch_bc(h, 0));
   int rc = transpose(h, false, 0, false);
   if (rc) return rc;
   FVM_CK(cudaMemcpyAsync(host_state, h->stage_dev, h->stage_elems * sizeof(double), cudaMemcpyDeviceToHost,
@@ -850,7 +862,7 @@ int fvm_download_async(fvm_handle* h, double* host_state) {
   if (!h || !host_state) return fail(FVM_E_INVALID, "null argument");
   int rc = ensure_async(h);
   if (rc) return rc;
-  FVM_CK(launch_bc(h, 0, false));
+  FVM_CK(launch_bc(h, 0));
   // the previous download's copy must have drained the staging buffer
   FVM_CK(cudaStreamWaitEvent(h->stream, h->ev_out_free, 0));
   if ((rc = transpose(h, false, 0, false, h->stage_out))) return rc;

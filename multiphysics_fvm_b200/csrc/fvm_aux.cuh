@@ -49,34 +49,6 @@ __device__ __forceinline__ void bc_fill_one(Real* __restrict__ u, const Layout& 
   }
 }
 
-// One grid's ghost faces: blockIdx.y = variable * 6 + side, blocks over the
-// face's rows b, threads along a row a (the (a, b) of bc_fill_one), so no
-// index is decoded by division.
-template <typename Real>
-__global__ void bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc, const int* active) {
-  if (active && !*active) return;
-  const int q = blockIdx.y / 6, side = blockIdx.y % 6;
-  if (q >= nv) return;
-  const int axis = side >> 1, high = side & 1;
-  const int A = axis == 0 ? L.ny : L.nx;  // along a row
-  const int B = axis == 2 ? L.ny : L.nz;  // rows
-  const int kind = bc.kind[q][side];
-  const int n = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
-  const int g = high ? n + 1 : 0;                       // ghost index along axis
-  const int inner = high ? n : 1;                       // adjacent interior
-  const int src = kind == 0 ? (high ? 1 : n) : inner;  // periodic: opposite layer
-  const Real two_w = Real(2) * Real(bc.value[q][side]);
-  for (int b = blockIdx.x; b < B; b += gridDim.x)
-    for (int a = threadIdx.x; a < A; a += blockDim.x) {
-      long long gi, si;
-      if (axis == 0) { gi = L.idx(q, b + 1, a + 1, g); si = L.idx(q, b + 1, a + 1, src); }
-      else if (axis == 1) { gi = L.idx(q, b + 1, g, a + 1); si = L.idx(q, b + 1, src, a + 1); }
-      else { gi = L.idx(q, g, b + 1, a + 1); si = L.idx(q, src, b + 1, a + 1); }
-      const Real v = u[si];
-      u[gi] = kind == 2 ? -v : (kind == 3 ? two_w - v : v);
-    }
-}
-
 // Reference layout (C order, last axis fastest) <-> device layout (x1 fastest).
 // src/dst reference arrays have dims (nv, m1, m2, m3) and map to ghosted device
 // indices g = m + off.  32x32 shared-memory tiles over (x1, x3) per (var, x2).
@@ -341,8 +313,57 @@ __device__ __forceinline__ void clock_one(Clock* clk, int mode, double max_inv_l
   clk->steps = clk->steps + 1;
 }
 
-__global__ void clock_kernel(Clock* clk, int mode, double max_inv_l2, double const_rate, unsigned* status) {
-  clock_one(clk, mode, max_inv_l2, const_rate, status);
+// The step's clock update (clock_one), when a ghost fill carries it.
+struct ClockArgs {
+  Clock* clk;  // null: the fill has no clock work
+  int mode;
+  double max_inv_l2, const_rate;
+  unsigned* status;
+};
+
+// One grid's ghost faces: blockIdx.y = variable * 6 + side; the face's cells
+// (a along the face row, b over rows) are dealt to the blocks of that grid row,
+// BCF per thread with every load issued before the stores: an x1 face is
+// strided (one sector per cell), so the fill is latency-bound and wants many
+// loads in flight.  The first fill of a step also closes the step's clock in
+// block (0, 0) (ck.clk set).  The fill does not read the clock: filling the
+// ghosts of a state whose step turns out to be a no-op changes nothing a
+// later read sees (the ghost faces are a function of the interior, and
+// downloads fill them again).
+constexpr int BCF = 4;
+template <typename Real>
+__global__ void __launch_bounds__(256) bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc, ClockArgs ck) {
+  if (ck.clk && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+    clock_one(ck.clk, ck.mode, ck.max_inv_l2, ck.const_rate, ck.status);
+  const int q = blockIdx.y / 6, side = blockIdx.y % 6;
+  if (q >= nv) return;
+  const int axis = side >> 1, high = side & 1;
+  const int A = axis == 0 ? L.ny : L.nx;  // along a row
+  const int B = axis == 2 ? L.ny : L.nz;  // rows
+  const int kind = bc.kind[q][side];
+  const int n = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
+  const int g = high ? n + 1 : 0;                       // ghost index along axis
+  const int inner = high ? n : 1;                       // adjacent interior
+  const int src = kind == 0 ? (high ? 1 : n) : inner;  // periodic: opposite layer
+  const Real two_w = Real(2) * Real(bc.value[q][side]);
+  const int total = A * B, stride = gridDim.x * blockDim.x;
+  for (int t0 = blockIdx.x * blockDim.x + threadIdx.x; t0 < total; t0 += BCF * stride) {
+    Real v[BCF];
+    long long gi[BCF];
+#pragma unroll
+    for (int m = 0; m < BCF; ++m) {
+      const int t = t0 + m * stride;
+      const int a = t % A, b = t / A;
+      long long si;
+      if (axis == 0) { gi[m] = L.idx(q, b + 1, a + 1, g); si = L.idx(q, b + 1, a + 1, src); }
+      else if (axis == 1) { gi[m] = L.idx(q, b + 1, g, a + 1); si = L.idx(q, b + 1, src, a + 1); }
+      else { gi[m] = L.idx(q, g, b + 1, a + 1); si = L.idx(q, src, b + 1, a + 1); }
+      v[m] = t < total ? u[si] : Real(0);
+    }
+#pragma unroll
+    for (int m = 0; m < BCF; ++m)
+      if (t0 + m * stride < total) u[gi[m]] = kind == 2 ? -v[m] : (kind == 3 ? two_w - v[m] : v[m]);
+  }
 }
 
 __global__ void batch_clock_kernel(const BatchAux* __restrict__ a, int n, int fixed) {
