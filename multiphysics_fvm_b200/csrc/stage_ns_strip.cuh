@@ -87,67 +87,37 @@ __device__ __forceinline__ float strip_slope(float a, float b) {
   else return flim_vanleer(a, b);
 }
 
-// Packed float32 pairs (sm_100 add/mul/fma.f32x2: two lanes per instruction).
-// A cell's six reconstructed fields are held as three pairs (rho, m1),
-// (m2, m3), (E, P); differences, face states and the flux combinations run on
-// the pairs, the limiters and the wave speeds per component.  Subtraction is
-// fma(b, -1, a), which rounds like a - b.
-__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-template <int LIM>
-__device__ __forceinline__ float2 strip_slope2(float2 a, float2 b) {
-  return make_float2(strip_slope<LIM>(a.x, b.x), strip_slope<LIM>(a.y, b.y));
-}
-// Limited slopes of the three pairs from the cells before (a), at (b) and
-// after (c) along one axis; zero on a ghost cell.
-template <int LIM>
-__device__ __forceinline__ void strip_slopes2(const float2* a, const float2* b, const float2* c, bool ghost, float2* s) {
-#pragma unroll
-  for (int k = 0; k < 3; ++k) s[k] = ghost ? make_float2(0.f, 0.f) : strip_slope2<LIM>(sub2(b[k], a[k]), sub2(c[k], b[k]));
-}
-
-// Inviscid Riemann flux along axis D from face states held as pairs
-// {(rho, m1), (m2, m3), (E, P)} (navier_stokes.py:159-214 fluxes, :280-355
-// wave speeds, riemann_solvers.py:13-89).  The Euler flux's mass component is
-// rho*v, the momentum rounded through 1/rho.
+// Inviscid Riemann flux along axis D from face states q = {rho, m1, m2, m3, E, P}
+// (navier_stokes.py:159-214 fluxes, :280-355 wave speeds).
 template <int D, int RIEM>
-__device__ __forceinline__ void strip_flux2(const float2* qL, const float2* qR, float gam, float* F) {
-  const float mL = D == 0 ? qL[0].y : (D == 1 ? qL[1].x : qL[1].y);
-  const float mR = D == 0 ? qR[0].y : (D == 1 ? qR[1].x : qR[1].y);
-  const float irL = rcp_approx(qL[0].x), irR = rcp_approx(qR[0].x);
-  const float vL = mL * irL, vR = mR * irR;
-  const float PL = qL[2].y, PR = qR[2].y;
-  const float cL = sqrt_approx((gam * PL) * irL), cR = sqrt_approx((gam * PR) * irR);
-  // Euler fluxes (rho v, m1 v), (m2 v, m3 v) + P on the axis momentum; (E + P) v
-  float2 FL0 = mul2(qL[0], bc2(vL)), FL1 = mul2(qL[1], bc2(vL));
-  float2 FR0 = mul2(qR[0], bc2(vR)), FR1 = mul2(qR[1], bc2(vR));
-  if constexpr (D == 0) { FL0.y += PL; FR0.y += PR; }
-  else if constexpr (D == 1) { FL1.x += PL; FR1.x += PR; }
-  else { FL1.y += PL; FR1.y += PR; }
-  const float FL4 = (qL[2].x + PL) * vL, FR4 = (qR[2].x + PR) * vR;
-  const float dE = qR[2].x - qL[2].x;
-  float2 G0, G1;
+__device__ __forceinline__ void strip_flux(const float* qL, const float* qR, float gam, float* F) {
+  const float irL = rcp_approx(qL[0]), irR = rcp_approx(qR[0]);
+  const float vL = qL[1 + D] * irL, vR = qR[1 + D] * irR;
+  const float cL = sqrt_approx((gam * qL[5]) * irL), cR = sqrt_approx((gam * qR[5]) * irR);
+  float FL[5], FR[5];
+  FL[0] = qL[1 + D];
+  FR[0] = qR[1 + D];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    FL[1 + c] = qL[1 + c] * vL;
+    FR[1 + c] = qR[1 + c] * vR;
+  }
+  FL[1 + D] += qL[5];
+  FR[1 + D] += qR[5];
+  FL[4] = (qL[4] + qL[5]) * vL;
+  FR[4] = (qR[4] + qR[5]) * vR;
   if constexpr (RIEM == RIEM_HLL) {
     const float sl = fminf(fminf(vL - cL, vR - cR), 0.f);
     const float sr = fmaxf(fmaxf(vL + cL, vR + cR), 0.f);
     const float rd = rcp_approx(fmaxf(sr - sl, 1e-30f));
     const float a = sr * rd, b = -sl * rd, c = (sl * sr) * rd;
-    G0 = fma2(bc2(a), FL0, fma2(bc2(b), FR0, mul2(bc2(c), sub2(qR[0], qL[0]))));
-    G1 = fma2(bc2(a), FL1, fma2(bc2(b), FR1, mul2(bc2(c), sub2(qR[1], qL[1]))));
-    F[4] = fmaf(a, FL4, fmaf(b, FR4, c * dE));
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F[v] = fmaf(a, FL[v], fmaf(b, FR[v], c * (qR[v] - qL[v])));
   } else {
     const float h = 0.5f * fmaxf(fabsf(vL) + cL, fabsf(vR) + cR);
-    G0 = fma2(bc2(0.5f), add2(FL0, FR0), mul2(bc2(-h), sub2(qR[0], qL[0])));
-    G1 = fma2(bc2(0.5f), add2(FL1, FR1), mul2(bc2(-h), sub2(qR[1], qL[1])));
-    F[4] = fmaf(0.5f, FL4 + FR4, -h * dE);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F[v] = fmaf(0.5f, FL[v] + FR[v], -h * (qR[v] - qL[v]));
   }
-  F[0] = G0.x;
-  F[1] = G0.y;
-  F[2] = G1.x;
-  F[3] = G1.y;
 }
 
 // P = (gamma - 1)(E - |m|^2 / (2 rho)) of one ring cell (navier_stokes.py:94-100).
@@ -213,12 +183,11 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
     // x3 state carried from step to step, per own cell: the left state of the
     // face above the last slope plane and the flux of the face below the
     // output plane
-    float2 qlz[R][3];
-    float fzp[R][5];
+    float qlz[R][NF], fzp[R][5];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) qlz[r][k] = make_float2(0.f, 0.f);
+      for (int f = 0; f < NF; ++f) qlz[r][f] = 0.f;
 #pragma unroll
       for (int v = 0; v < 5; ++v) fzp[r][v] = 0.f;
     }
@@ -256,14 +225,13 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
         if (outstep) {
           const int par = K & 1;
           const int jb = y0 + w * R;  // first row of the strip
-          // the six fields of ring cell (row ty, column tx) as three pairs
-          auto ldf = [&](float2* f, int ty, int tx) {
+          auto ldf = [&](float* f, int ty, int tx) {
             const int o = (ty + HH) * W + tx + 4;
-            f[0] = make_float2(uK[o], uK[PL + o]);
-            f[1] = make_float2(uK[2 * PL + o], uK[3 * PL + o]);
-            f[2] = make_float2(uK[4 * PL + o], pK[(ty + 2) * W2 + tx + 2]);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) f[v] = uK[v * PL + o];
+            f[5] = pK[(ty + 2) * W2 + tx + 2];
           };
-          float2 fa[3], fb[3], fc[3], ql[3];
+          float fa[NF], fb[NF], fc[NF], ql[NF];
           ldf(fa, w * R - 2, lane);
           ldf(fb, w * R - 1, lane);
 #pragma unroll
@@ -274,14 +242,15 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
             const int ty = w * R - 1 + t;
             const int j = jb - 1 + t;
             ldf(fc, ty + 1, lane);
-            float2 s[3];
-            strip_slopes2<LIM>(fa, fb, fc, j < 0 || j >= ny, s);
-            if (t >= 1) {
-              float2 qr[3];
-              float F[5];
+            const bool yghost = j < 0 || j >= ny;
+            float s[NF];
 #pragma unroll
-              for (int k = 0; k < 3; ++k) qr[k] = fma2(bc2(-0.5f), s[k], fb[k]);
-              strip_flux2<1, RIEM>(ql, qr, gam, F);
+            for (int f = 0; f < NF; ++f) s[f] = yghost ? 0.f : strip_slope<LIM>(fb[f] - fa[f], fc[f] - fb[f]);
+            if (t >= 1) {
+              float qr[NF], F[5];
+#pragma unroll
+              for (int f = 0; f < NF; ++f) qr[f] = fmaf(-0.5f, s[f], fb[f]);
+              strip_flux<1, RIEM>(ql, qr, gam, F);
               if (t >= 2) {
                 const float idym = __ldg(p.met.inv_dx2 + min(max(j - 1, 0), ny - 1));
 #pragma unroll
@@ -294,29 +263,24 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
               }
             }
 #pragma unroll
-            for (int k = 0; k < 3; ++k) ql[k] = fma2(bc2(0.5f), s[k], fb[k]);
+            for (int f = 0; f < NF; ++f) ql[f] = fmaf(0.5f, s[f], fb[f]);
             if (t >= 1 && t <= R) {
               // x1 for own row r = t - 1 (cell i, row j): the flux through
               // the cell's left face, the right face's from the next lane
               const int r = t - 1;
-              float2 fm[3], fp[3], s1[3], qlx[3], qrx[3];
-              float F[5];
+              float fm[NF], fp[NF], qlx[NF], qrx[NF], F[5];
               ldf(fm, ty, lane - 1);
               ldf(fp, ty, lane + 1);
-              strip_slopes2<LIM>(fm, fb, fp, i >= nx, s1);  // i == nx: the right ghost column
+              const bool xghost = i >= nx;  // i == nx: the right ghost column
 #pragma unroll
-              for (int k = 0; k < 3; ++k) {
-                float2 sl;
-                sl.x = __shfl_up_sync(0xffffffffu, s1[k].x, 1);
-                sl.y = __shfl_up_sync(0xffffffffu, s1[k].y, 1);
-                if (lane == 0) {
-                  sl.x = hl[(par * NF + 2 * k) * TY + ty];
-                  sl.y = hl[(par * NF + 2 * k + 1) * TY + ty];
-                }
-                qlx[k] = fma2(bc2(0.5f), sl, fm[k]);
-                qrx[k] = fma2(bc2(-0.5f), s1[k], fb[k]);
+              for (int f = 0; f < NF; ++f) {
+                const float s1 = xghost ? 0.f : strip_slope<LIM>(fb[f] - fm[f], fp[f] - fb[f]);
+                const float su = __shfl_up_sync(0xffffffffu, s1, 1);
+                const float sl = lane == 0 ? hl[(par * NF + f) * TY + ty] : su;
+                qlx[f] = fmaf(0.5f, sl, fm[f]);
+                qrx[f] = fmaf(-0.5f, s1, fb[f]);
               }
-              strip_flux2<0, RIEM>(qlx, qrx, gam, F);
+              strip_flux<0, RIEM>(qlx, qrx, gam, F);
 #pragma unroll
               for (int v = 0; v < 5; ++v) {
                 const float fd = __shfl_down_sync(0xffffffffu, F[v], 1);
@@ -325,7 +289,7 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
               }
             }
 #pragma unroll
-            for (int k = 0; k < 3; ++k) { fa[k] = fb[k]; fb[k] = fc[k]; }
+            for (int f = 0; f < NF; ++f) { fa[f] = fb[f]; fb[f] = fc[f]; }
           }
         }
       } else {
@@ -338,39 +302,37 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
         const int j = y0 + row;
         if (Kh >= Z0 && Kh <= Zl && lane < 2 * TY && j < ny) {
           const int hpar = Kh & 1;
-          auto ldh = [&](float2* f, int tx) {
+          auto ldh = [&](float* f, int tx) {
             const int o = (row + HH) * W + tx + 4;
-            f[0] = make_float2(uK1[o], uK1[PL + o]);
-            f[1] = make_float2(uK1[2 * PL + o], uK1[3 * PL + o]);
-            f[2] = make_float2(uK1[4 * PL + o], pK1[(row + 2) * W2 + tx + 2]);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) f[v] = uK1[v * PL + o];
+            f[5] = pK1[(row + 2) * W2 + tx + 2];
           };
           if (lane < TY) {
-            float2 a[3], b[3], c[3], sl[3];
+            float a[NF], b[NF], c[NF];
             ldh(a, -2);
             ldh(b, -1);
             ldh(c, 0);
-            strip_slopes2<LIM>(a, b, c, x0 == 0, sl);  // zero on the left ghost column
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-              hl[(hpar * NF + 2 * k) * TY + row] = sl[k].x;
-              hl[(hpar * NF + 2 * k + 1) * TY + row] = sl[k].y;
-            }
+            for (int f = 0; f < NF; ++f)  // zero on the left ghost column
+              hl[(hpar * NF + f) * TY + row] = x0 == 0 ? 0.f : strip_slope<LIM>(b[f] - a[f], c[f] - b[f]);
           } else {
             float F[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
             if (x0 + TX <= nx) {  // the face between x0 + 31 and x0 + 32 is needed
-              float2 a[3], b[3], c[3], d[3], sm1[3], s0[3], ql[3], qr[3];
+              float a[NF], b[NF], c[NF], d[NF], ql[NF], qr[NF];
               ldh(a, TX - 2);
               ldh(b, TX - 1);
               ldh(c, TX);
               ldh(d, TX + 1);
-              strip_slopes2<LIM>(a, b, c, false, sm1);
-              strip_slopes2<LIM>(b, c, d, x0 + TX >= nx, s0);  // x0 + 32 may be the right ghost column
+              const bool g32 = x0 + TX >= nx;  // x0 + 32 is the right ghost column
 #pragma unroll
-              for (int k = 0; k < 3; ++k) {
-                ql[k] = fma2(bc2(0.5f), sm1[k], b[k]);
-                qr[k] = fma2(bc2(-0.5f), s0[k], c[k]);
+              for (int f = 0; f < NF; ++f) {
+                const float sm1 = strip_slope<LIM>(b[f] - a[f], c[f] - b[f]);
+                const float s0 = g32 ? 0.f : strip_slope<LIM>(c[f] - b[f], d[f] - c[f]);
+                ql[f] = fmaf(0.5f, sm1, b[f]);
+                qr[f] = fmaf(-0.5f, s0, c[f]);
               }
-              strip_flux2<0, RIEM>(ql, qr, gam, F);
+              strip_flux<0, RIEM>(ql, qr, gam, F);
             }
 #pragma unroll
             for (int v = 0; v < 5; ++v) fr[(hpar * 5 + v) * TY + row] = F[v];
@@ -419,22 +381,19 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
         for (int r = 0; r < R; ++r) {
           const int ty = w * R + r;
           const int o = (ty + HH) * W + lane + 4, op = (ty + 2) * W2 + lane + 2;
-          float2 a0[3], a1[3], a2[3], sz[3], qr[3];
-          a0[0] = make_float2(uK[o], uK[PL + o]);
-          a0[1] = make_float2(uK[2 * PL + o], uK[3 * PL + o]);
-          a0[2] = make_float2(uK[4 * PL + o], pK[op]);
-          a1[0] = make_float2(uK1[o], uK1[PL + o]);
-          a1[1] = make_float2(uK1[2 * PL + o], uK1[3 * PL + o]);
-          a1[2] = make_float2(uK1[4 * PL + o], pK1[op]);
-          a2[0] = make_float2(uK2[o], uK2[PL + o]);
-          a2[1] = make_float2(uK2[2 * PL + o], uK2[3 * PL + o]);
-          a2[2] = make_float2(uK2[4 * PL + o], pnew[r]);
-          strip_slopes2<LIM>(a0, a1, a2, zghost, sz);
+          float qr[NF], qn[NF];
 #pragma unroll
-          for (int k = 0; k < 3; ++k) qr[k] = fma2(bc2(-0.5f), sz[k], a1[k]);
+          for (int f = 0; f < NF; ++f) {
+            const float a0 = f < 5 ? uK[f * PL + o] : pK[op];
+            const float a1 = f < 5 ? uK1[f * PL + o] : pK1[op];
+            const float a2 = f < 5 ? uK2[f * PL + o] : pnew[r];
+            const float s = zghost ? 0.f : strip_slope<LIM>(a1 - a0, a2 - a1);
+            qr[f] = fmaf(-0.5f, s, a1);
+            qn[f] = fmaf(0.5f, s, a1);
+          }
           if (zface) {
             float F[5];
-            strip_flux2<2, RIEM>(qlz[r], qr, gam, F);
+            strip_flux<2, RIEM>(qlz[r], qr, gam, F);
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
               kv[r][v] = fmaf(F[v] - fzp[r][v], idz, kv[r][v]);
@@ -442,7 +401,7 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
             }
           }
 #pragma unroll
-          for (int k = 0; k < 3; ++k) qlz[r][k] = fma2(bc2(0.5f), sz[k], a1[k]);
+          for (int f = 0; f < NF; ++f) qlz[r][f] = qn[f];
         }
         // ------------------------------------------------------------ 6 ----
         if (outstep) {
