@@ -531,9 +531,9 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
   // the first stage's ghost fill also closes the clock (dt, t, step count, active)
   const int cmode = dt_mode == 1 ? 1 : (state_dt ? 0 : 2);
   const ClockArgs ck{h->clk, cmode, h->max_inv_l2, h->const_rate, h->status};
+  const std::vector<StageDef> stages = stage_table(h->d.integrator);
   {
-    const StageDef& s0 = stage_table(h->d.integrator).front();
-    cudaError_t e = launch_bc(h, s0.in, &ck);
+    cudaError_t e = launch_bc(h, stages.front().in, &ck);
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
   }
   if (h->closure) {
@@ -543,7 +543,7 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("closure: ") + cudaGetErrorString(e));
   }
   bool first = true;
-  for (const StageDef& sd : stage_table(h->d.integrator)) {
+  for (const StageDef& sd : stages) {
     cudaError_t e = first ? cudaSuccess : launch_bc(h, sd.in);
     first = false;
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));

@@ -165,7 +165,10 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
     const int x0 = tx_i * TX, y0 = ty_i * TY;
     const int Z0 = 1 + zc_i * p.zchunk;         // first ghosted output plane
     const int Zl = min(Z0 + p.zchunk - 1, nz);  // last ghosted output plane
-    const int Kfirst = Z0 - 2, Plast = Zl + HH;
+    // a one-plane grid whose x3 ghosts copy the plane ("flat") has x3 fluxes
+    // that cancel exactly: plane 1 alone, no x3 pipeline
+    const bool flat = p.flat != 0;
+    const int Kfirst = flat ? Z0 : Z0 - 2, Plast = flat ? Zl : Zl + HH;
     const int i = x0 + lane;
     const float idx = (is_out && i < nx) ? __ldg(p.met.inv_dx1 + i) : 0.f;
 
@@ -176,9 +179,74 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
       mbar_arrive_expect_tx(&bars[s], C::TX_BYTES + p.extra_tx);
       tma_load_4d(&uring[s * C::SLOT], tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
     };
-    // planes Kfirst .. Kfirst + 2 (the first step's)
+    // planes Kfirst .. Kfirst + 2 (the first step's; a flat grid's one plane)
     if (tid == 0)
-      for (int pl = Kfirst; pl <= Kfirst + 2; ++pl) issue(pl);
+      for (int pl = Kfirst; pl <= (flat ? Kfirst : Kfirst + 2); ++pl) issue(pl);
+
+    // Halo warp: x1 data of plane Kh (ring plane uH, P plane pH) outside the
+    // warps: lanes 0..TY-1 the slopes of the cell left of the tile, lanes
+    // TY..2TY-1 the flux through the tile's right edge
+    auto halo_x1 = [&](int Kh, const float* uH, const float* pH) {
+      const int row = lane < TY ? lane : lane - TY;
+      const int j = y0 + row;
+      if (Kh >= Z0 && Kh <= Zl && lane < 2 * TY && j < ny) {
+        const int hpar = Kh & 1;
+        auto ldh = [&](float* f, int tx) {
+          const int o = (row + HH) * W + tx + 4;
+#pragma unroll
+          for (int v = 0; v < 5; ++v) f[v] = uH[v * PL + o];
+          f[5] = pH[(row + 2) * W2 + tx + 2];
+        };
+        if (lane < TY) {
+          float a[NF], b[NF], c[NF];
+          ldh(a, -2);
+          ldh(b, -1);
+          ldh(c, 0);
+#pragma unroll
+          for (int f = 0; f < NF; ++f)  // zero on the left ghost column
+            hl[(hpar * NF + f) * TY + row] = x0 == 0 ? 0.f : strip_slope<LIM>(b[f] - a[f], c[f] - b[f]);
+        } else {
+          float F[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+          if (x0 + TX <= nx) {  // the face between x0 + 31 and x0 + 32 is needed
+            float a[NF], b[NF], c[NF], d[NF], ql[NF], qr[NF];
+            ldh(a, TX - 2);
+            ldh(b, TX - 1);
+            ldh(c, TX);
+            ldh(d, TX + 1);
+            const bool g32 = x0 + TX >= nx;  // x0 + 32 is the right ghost column
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+              const float sm1 = strip_slope<LIM>(b[f] - a[f], c[f] - b[f]);
+              const float s0 = g32 ? 0.f : strip_slope<LIM>(c[f] - b[f], d[f] - c[f]);
+              ql[f] = fmaf(0.5f, sm1, b[f]);
+              qr[f] = fmaf(-0.5f, s0, c[f]);
+            }
+            strip_flux<0, RIEM>(ql, qr, gam, F);
+          }
+#pragma unroll
+          for (int v = 0; v < 5; ++v) fr[(hpar * 5 + v) * TY + row] = F[v];
+        }
+      }
+    };
+    // Halo warp: P of ring plane usrc on the cells of the P plane no output
+    // thread owns
+    auto border_p = [&](float* pdst, const float* usrc) {
+      for (int b = lane; b < C::NBORDER; b += 32) {
+        int x, y;
+        if (b < 2 * W2) {
+          y = b / W2 - 2;
+          x = b % W2 - 2;
+        } else if (b < 4 * W2) {
+          y = TY + (b - 2 * W2) / W2;
+          x = (b - 2 * W2) % W2 - 2;
+        } else {
+          const int c = b - 4 * W2;
+          y = c >> 2;
+          x = (c & 3) < 2 ? (c & 3) - 2 : (c & 3) + 30;
+        }
+        pdst[(y + 2) * W2 + x + 2] = strip_pressure(usrc + (y + HH) * W + x + 4, PL, gm1);
+      }
+    };
 
     // x3 state carried from step to step, per own cell: the left state of the
     // face above the last slope plane and the flux of the face below the
@@ -220,6 +288,29 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
       for (int r = 0; r < R; ++r)
 #pragma unroll
         for (int v = 0; v < 5; ++v) kv[r][v] = 0.f;
+      if (flat) {
+        // the plane itself, its P over the tile + 2 and the halo warp's x1
+        // data, before the sweep
+        const bool g = mbar_wait_bounded(&bars[sK], (phase_bits >> sK) & 1u, p.wait_ns);
+        if (g) {
+          phase_bits ^= 1u << sK;
+          if (tid == 0) pending &= ~(1u << sK);
+          if (is_out) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int ty = w * R + r;
+              pK[(ty + 2) * W2 + lane + 2] = strip_pressure(uK + (ty + HH) * W + lane + 4, PL, gm1);
+            }
+          } else {
+            border_p(pK, uK);
+          }
+        } else {
+          atomicOr(p.status, ST_TMA_TIMEOUT);
+        }
+        if (!__syncthreads_and(g)) return false;
+        if (!is_out) halo_x1(K, uK, pK);
+        __syncthreads();
+      }
       // ------------------------------------------------------------ 2 ----
       if (is_out) {
         if (outstep) {
@@ -294,50 +385,9 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
         }
       } else {
         // --------------------------------------------------- halo warp ----
-        // x1 data of plane K+1 (the next output plane) outside the warps:
-        // lanes 0..TY-1 the slopes of the cell left of the tile, lanes
-        // TY..2TY-1 the flux through the tile's right edge
-        const int Kh = K + 1;
-        const int row = lane < TY ? lane : lane - TY;
-        const int j = y0 + row;
-        if (Kh >= Z0 && Kh <= Zl && lane < 2 * TY && j < ny) {
-          const int hpar = Kh & 1;
-          auto ldh = [&](float* f, int tx) {
-            const int o = (row + HH) * W + tx + 4;
-#pragma unroll
-            for (int v = 0; v < 5; ++v) f[v] = uK1[v * PL + o];
-            f[5] = pK1[(row + 2) * W2 + tx + 2];
-          };
-          if (lane < TY) {
-            float a[NF], b[NF], c[NF];
-            ldh(a, -2);
-            ldh(b, -1);
-            ldh(c, 0);
-#pragma unroll
-            for (int f = 0; f < NF; ++f)  // zero on the left ghost column
-              hl[(hpar * NF + f) * TY + row] = x0 == 0 ? 0.f : strip_slope<LIM>(b[f] - a[f], c[f] - b[f]);
-          } else {
-            float F[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-            if (x0 + TX <= nx) {  // the face between x0 + 31 and x0 + 32 is needed
-              float a[NF], b[NF], c[NF], d[NF], ql[NF], qr[NF];
-              ldh(a, TX - 2);
-              ldh(b, TX - 1);
-              ldh(c, TX);
-              ldh(d, TX + 1);
-              const bool g32 = x0 + TX >= nx;  // x0 + 32 is the right ghost column
-#pragma unroll
-              for (int f = 0; f < NF; ++f) {
-                const float sm1 = strip_slope<LIM>(b[f] - a[f], c[f] - b[f]);
-                const float s0 = g32 ? 0.f : strip_slope<LIM>(c[f] - b[f], d[f] - c[f]);
-                ql[f] = fmaf(0.5f, sm1, b[f]);
-                qr[f] = fmaf(-0.5f, s0, c[f]);
-              }
-              strip_flux<0, RIEM>(ql, qr, gam, F);
-            }
-#pragma unroll
-            for (int v = 0; v < 5; ++v) fr[(hpar * 5 + v) * TY + row] = F[v];
-          }
-        }
+        // x1 data of plane K+1, the next output plane (a flat grid's was
+        // formed before the sweep)
+        if (!flat) halo_x1(K + 1, uK1, pK1);
       }
       // ------------------------------------------------------------ 3 ----
       // Every thread waits for the plane itself; nothing read after the wait
@@ -345,7 +395,7 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
       // barrier here.  A thread whose wait ran out skips the rest of the step
       // and the barrier at its end takes the block out.
       bool got = true;
-      for (int pl = (K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
+      for (int pl = (K == Kfirst ? Kfirst : K + 2); !flat && pl <= K + 2; ++pl) {
         const int s = pmod(pl, C::NSLOT);
         const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
         if (g) {
@@ -359,49 +409,51 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
       if (!got) {
         // skip to the barrier
       } else if (is_out) {
-        // ------------------------------------------------------------ 4 ----
-        float pnew[R];
+        if (!flat) {  // x3 (a flat grid has none)
+          // ------------------------------------------------------------ 4 ----
+          float pnew[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int ty = w * R + r;
-          const int o = (ty + HH) * W + lane + 4, op = (ty + 2) * W2 + lane + 2;
-          pnew[r] = strip_pressure(uK2 + o, PL, gm1);
-          pK2[op] = pnew[r];
-          if (K == Kfirst) {
-            pK[op] = strip_pressure(uK + o, PL, gm1);
-            pK1[op] = strip_pressure(uK1 + o, PL, gm1);
-          }
-        }
-        // ------------------------------------------------------------ 5 ----
-        // slope of plane K+1 (zero on a ghost plane) and the flux at K+1/2
-        const bool zghost = K + 1 <= 0 || K + 1 >= nz + 1;
-        const bool zface = K >= Z0 - 1;
-        const float idz = outstep ? __ldg(p.met.inv_dx3 + (K - 1)) : 0.f;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int ty = w * R + r;
-          const int o = (ty + HH) * W + lane + 4, op = (ty + 2) * W2 + lane + 2;
-          float qr[NF], qn[NF];
-#pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            const float a0 = f < 5 ? uK[f * PL + o] : pK[op];
-            const float a1 = f < 5 ? uK1[f * PL + o] : pK1[op];
-            const float a2 = f < 5 ? uK2[f * PL + o] : pnew[r];
-            const float s = zghost ? 0.f : strip_slope<LIM>(a1 - a0, a2 - a1);
-            qr[f] = fmaf(-0.5f, s, a1);
-            qn[f] = fmaf(0.5f, s, a1);
-          }
-          if (zface) {
-            float F[5];
-            strip_flux<2, RIEM>(qlz[r], qr, gam, F);
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-              kv[r][v] = fmaf(F[v] - fzp[r][v], idz, kv[r][v]);
-              fzp[r][v] = F[v];
+          for (int r = 0; r < R; ++r) {
+            const int ty = w * R + r;
+            const int o = (ty + HH) * W + lane + 4, op = (ty + 2) * W2 + lane + 2;
+            pnew[r] = strip_pressure(uK2 + o, PL, gm1);
+            pK2[op] = pnew[r];
+            if (K == Kfirst) {
+              pK[op] = strip_pressure(uK + o, PL, gm1);
+              pK1[op] = strip_pressure(uK1 + o, PL, gm1);
             }
           }
+          // ------------------------------------------------------------ 5 ----
+          // slope of plane K+1 (zero on a ghost plane) and the flux at K+1/2
+          const bool zghost = K + 1 <= 0 || K + 1 >= nz + 1;
+          const bool zface = K >= Z0 - 1;
+          const float idz = outstep ? __ldg(p.met.inv_dx3 + (K - 1)) : 0.f;
 #pragma unroll
-          for (int f = 0; f < NF; ++f) qlz[r][f] = qn[f];
+          for (int r = 0; r < R; ++r) {
+            const int ty = w * R + r;
+            const int o = (ty + HH) * W + lane + 4, op = (ty + 2) * W2 + lane + 2;
+            float qr[NF], qn[NF];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+              const float a0 = f < 5 ? uK[f * PL + o] : pK[op];
+              const float a1 = f < 5 ? uK1[f * PL + o] : pK1[op];
+              const float a2 = f < 5 ? uK2[f * PL + o] : pnew[r];
+              const float s = zghost ? 0.f : strip_slope<LIM>(a1 - a0, a2 - a1);
+              qr[f] = fmaf(-0.5f, s, a1);
+              qn[f] = fmaf(0.5f, s, a1);
+            }
+            if (zface) {
+              float F[5];
+              strip_flux<2, RIEM>(qlz[r], qr, gam, F);
+#pragma unroll
+              for (int v = 0; v < 5; ++v) {
+                kv[r][v] = fmaf(F[v] - fzp[r][v], idz, kv[r][v]);
+                fzp[r][v] = F[v];
+              }
+            }
+#pragma unroll
+            for (int f = 0; f < NF; ++f) qlz[r][f] = qn[f];
+          }
         }
         // ------------------------------------------------------------ 6 ----
         if (outstep) {
@@ -445,25 +497,13 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
           if (bad) atomicOr(p.status, bad);
         }
       } else {
-        // P of plane K+2 on the cells of the P plane no output thread owns
-        for (int b = lane; b < C::NBORDER; b += 32) {
-          int x, y;
-          if (b < 2 * W2) {
-            y = b / W2 - 2;
-            x = b % W2 - 2;
-          } else if (b < 4 * W2) {
-            y = TY + (b - 2 * W2) / W2;
-            x = (b - 2 * W2) % W2 - 2;
-          } else {
-            const int c = b - 4 * W2;
-            y = c >> 2;
-            x = (c & 3) < 2 ? (c & 3) - 2 : (c & 3) + 30;
-          }
-          const int o = (y + HH) * W + x + 4, op = (y + 2) * W2 + x + 2;
-          pK2[op] = strip_pressure(uK2 + o, PL, gm1);
+        // P of plane K+2 (and on the first step of K, K+1) on the cells of
+        // the P plane no output thread owns
+        if (!flat) {
+          border_p(pK2, uK2);
           if (K == Kfirst) {
-            pK[op] = strip_pressure(uK + o, PL, gm1);
-            pK1[op] = strip_pressure(uK1 + o, PL, gm1);
+            border_p(pK, uK);
+            border_p(pK1, uK1);
           }
         }
       }
