@@ -244,10 +244,10 @@ __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, co
         const double cs = sqrt((gam * P) * ir);
         if (!(rho > 0.0)) bad |= ST_DENSITY;
         if (!(P > 0.0)) bad |= ST_PRESSURE;
-        const double vv[3] = {v0, v1, v2};
-        double ml[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) ml[d] = fmax(fmax(fabs(vv[d] + 0.0), fabs(vv[d] + (-cs))), fabs(vv[d] + cs));
+        // max(|v|, |v - c|, |v + c|) of the reference's three waves is
+        // fl(|v| + c) for c >= 0: |v - c| and |v + c| are |v| -+ c up to sign,
+        // and rounding is monotone
+        const double ml[3] = {fabs(v0) + cs, fabs(v1) + cs, fabs(v2) + cs};
         const double r = fmax(fmax(ml[0] * inv_len<double, COORD, 0>(m, i, j, k), ml[1] * inv_len<double, COORD, 1>(m, i, j, k)),
                               ml[2] * inv_len<double, COORD, 2>(m, i, j, k));
         const double nl = mu * ir;
