@@ -204,6 +204,21 @@ def closure_line():
         return {"error": f"{type(e).__name__}: {e}"}
 
 
+def profile_traffic(name):
+    """DRAM bytes per stage launch at 256^3 and their source, from the
+    machine-readable lines of a committed ncu summary (profiles/); not measured
+    in this run."""
+    traffic, source = None, None
+    tp = os.path.join(ROOT, "profiles", name)
+    if os.path.exists(tp):
+        for line in open(tp):
+            if "traffic_bytes_per_launch_256:" in line:
+                traffic = float(line.split("traffic_bytes_per_launch_256:")[1].split()[0])
+            if "traffic_source:" in line:
+                source = line.split("traffic_source:")[1].strip().rstrip("->").strip()
+    return traffic, source
+
+
 # North-star kernel: 3D Kelvin-Helmholtz, inviscid, MUSCL minmod + HLL + SSPRK3
 # at 256^3 in float32.  SSPRK3 stage launches move R1W1, R2W1, R2W1 field passes
 # of 5 float32 variables; the CFL reduction reads the state once.
@@ -229,6 +244,7 @@ def kh3d_line(steps, warmup, peak, peak_source):
         status = sim.status()
         tile_ty, _ = sim.tiling()
         sim.close()
+        kh_traffic, kh_source = profile_traffic("ns_strip_kh3d_256.md")
         cells = N_SIDE ** 3
         ms_step = ms / steps
         per_launch = stage_ms / launches
@@ -243,7 +259,8 @@ def kh3d_line(steps, warmup, peak, peak_source):
                 "step_breakdown_ms": {"stage_kernels": stage_ms / nst, "other_kernels": other_ms / nst},
                 "step_gbs": step_gbs, "step_frac": step_gbs / peak,
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                             "traffic": None, "kernel": "NS stage kernel (fused residual + SSPRK3 stage)",
+                             "traffic": kh_traffic, "traffic_source": kh_source,
+                             "kernel": "NS stage kernel (fused residual + SSPRK3 stage)",
                              "per_launch_ms": per_launch, "alg_bytes_per_launch": alg_launch,
                              "bytes_per_cell_update": sum(KH_STAGE_BYTES) + DT_BYTES,
                              "peak_source": peak_source}}
@@ -295,14 +312,7 @@ def run_ours(args):
     peak_source = "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650"
     # DRAM bytes per stage launch: not measured in this run; read from the
     # committed ncu capture (profiles/) and labelled with its source
-    traffic, traffic_source = None, None
-    tp = os.path.join(ROOT, "profiles", "ns_stage_rt3d_256.md")
-    if os.path.exists(tp):
-        for line in open(tp):
-            if "traffic_bytes_per_launch_256:" in line:
-                traffic = float(line.split("traffic_bytes_per_launch_256:")[1].split()[0])
-            if "traffic_source:" in line:
-                traffic_source = line.split("traffic_source:")[1].strip().rstrip("->").strip()
+    traffic, traffic_source = profile_traffic("ns_stage_rt3d_256.md")
 
     # end to end through the public API with host buffers: every step uploads
     # the float64 ghosted state from pinned memory, advances one step and
