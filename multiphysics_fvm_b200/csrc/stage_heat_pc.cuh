@@ -118,21 +118,22 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
           if (need_acc) eacc[r] = p.acc[g];
         }
       }
-      // Every thread waits for the planes itself; nothing read in the step was
-      // written by another thread, so only the barrier at the end of the step
-      // orders the block.  A thread whose wait ran out skips the step's work and
-      // that barrier takes the block out.
-      bool got = true;
-      for (int pl = (K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
-        const int s = pmod(pl, C::NSLOT);
-        const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
-        if (g) {
-          phase_bits ^= 1u << s;
-          if (tid == 0) pending &= ~(1u << s);
+      {
+        bool got = true;
+        for (int pl = (K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
+          const int s = pmod(pl, C::NSLOT);
+          const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
+          if (g) {
+            phase_bits ^= 1u << s;
+            if (tid == 0) pending &= ~(1u << s);
+          }
+          got = g;
         }
-        got = g;
+        if (!__syncthreads_and(got)) {
+          if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+          return false;
+        }
       }
-      if (!got) atomicOr(p.status, ST_TMA_TIMEOUT);
       const int s2 = sK + 2 >= C::NSLOT ? sK + 2 - C::NSLOT : sK + 2;
       const float* uK = uring + sK * C::SLOT;
       const float* uK2 = uring + s2 * C::SLOT;
@@ -144,9 +145,9 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int o = (w * R + r + HH) * W + lane + 4;
-        phz2[r] = got ? (g3[r] * idz1) * (uK2[o] - uK[o]) : 0.f;
+        phz2[r] = (g3[r] * idz1) * (uK2[o] - uK[o]);
       }
-      if (outstep && got) {
+      if (outstep) {
         const float idz = __ldg(m.inv_dx3 + (K - 1));
         // x2: phi2 along the strip (rows jb-1 .. jb+R) from the ring
         float ph2[R + 2];
@@ -183,15 +184,14 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
         phz0[r] = phz1[r];
         phz1[r] = phz2[r];
       }
-      if (!__syncthreads_and(got)) return false;  // plane K's slot is refilled at the next step
+      __syncthreads();  // plane K's slot is refilled at the next step
     }
   }
   return true;
 }
 
-// 768 resident threads per SM (6 blocks of 4 warps): at most 80 registers.
 template <int COORD, int R, int NW>
-__global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT, 768 / HeatPcCfg<R, NW>::NT)
+__global__ void __launch_bounds__(HeatPcCfg<R, NW>::NT)
     heat_pc_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ HeatParams<float> p) {
   using C = HeatPcCfg<R, NW>;
   extern __shared__ __align__(128) unsigned char smem_raw[];

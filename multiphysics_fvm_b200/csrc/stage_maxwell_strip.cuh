@@ -359,31 +359,30 @@ __global__ void __launch_bounds__(MxStripCfg<R, NW>::NT, MINB)
         }
       }
       // ------------------------------------------------------------ 3 ----
-      // Every thread waits for the plane itself; nothing read after the wait
-      // was written by another thread in this step (the residual ring plane
-      // formed now is read at the next step), so the block needs no barrier
-      // here.  A thread whose wait ran out skips the rest of the step and the
-      // barrier at its end takes the block out.
-      bool got = true;
-      for (int pl = (K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
-        const int s = pmod(pl, C::NSLOT);
-        const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
-        if (g) {
-          phase_bits ^= 1u << s;
-          if (tid == 0) pending &= ~(1u << s);
+      {
+        bool got = true;
+        for (int pl = (K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
+          const int s = pmod(pl, C::NSLOT);
+          const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
+          if (g) {
+            phase_bits ^= 1u << s;
+            if (tid == 0) pending &= ~(1u << s);
+          }
+          got = g;
         }
-        got = g;
+        if (!__syncthreads_and(got)) {
+          if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+          ok = false;
+          break;
+        }
       }
-      if (!got) atomicOr(p.status, ST_TMA_TIMEOUT);
       // ------------------------------------------------------------ 4 ----
       // cleaning residuals of plane K+1 (interior cells of the tile + 1)
       const int kr = K;  // interior index of plane K+1
       const bool rplane = kr >= 0 && kr < nz;
       float rown[R][2];
-      bool step_ok = got;
-      if (!got) {
-        // skip to the barrier
-      } else if (is_out) {
+      bool step_ok = true;
+      if (is_out) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int ty = w * R + r, j = jb + r;
@@ -433,7 +432,7 @@ __global__ void __launch_bounds__(MxStripCfg<R, NW>::NT, MINB)
               if (tid == 0) pending &= ~(1u << C::NSLOT);
             }
           }
-          step_ok = step_ok && staged_ok;
+          step_ok = staged_ok;
           unsigned bad = staged_ok ? 0u : ST_TMA_TIMEOUT;
           const float h3k = idz;  // 0.5/L3 = g3 * idz
 #pragma unroll
