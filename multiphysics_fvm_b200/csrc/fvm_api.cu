@@ -373,17 +373,6 @@ bool flat_grid(const fvm_handle* h) {
   return true;
 }
 
-// x1 sides (bit s) whose ghost faces the piecewise-constant heat kernel forms
-// in its TMA ring during steps (non-periodic sides); the step's ghost fills
-// skip them.
-int x1_ring_sides(const fvm_handle* h) {
-  if (!heat_pc_kernel(h)) return 0;
-  int m = 0;
-  for (int s = 0; s < 2; ++s)
-    if (h->d.bc_kind[0][s] != FVM_BC_PERIODIC) m |= 1 << s;
-  return m;
-}
-
 template <typename Real>
 NsParams<Real> make_ns_params(fvm_handle* h, const StageDef& sd, bool rhs_only) {
   const fvm_desc& d = h->d;
@@ -407,13 +396,6 @@ HeatParams<Real> make_heat_params(fvm_handle* h, const StageDef& sd, bool rhs_on
   p.inv_rho_cp = 1.0 / (d.params[0] * d.params[1]);
   p.k = d.params[2];
   p.q = d.params[3];
-  // steps of the piecewise-constant kernel form non-periodic x1 ghost faces in
-  // their TMA ring; the residual alone uses the ghosts it was given
-  p.x1patch = rhs_only ? 0 : x1_ring_sides(h);
-  for (int s = 0; s < 2; ++s) {
-    p.x1kind[s] = d.bc_kind[0][s];
-    p.x1w2[s] = float(2.0 * d.bc_value[0][s]);
-  }
   return p;
 }
 
@@ -474,7 +456,7 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
 }
 
 // Ghost fill of state buffer b; `ck` (optional) also closes the step's clock.
-cudaError_t launch_bc(fvm_handle* h, int b, const ClockArgs* ck = nullptr, int skip_x1 = 0) {
+cudaError_t launch_bc(fvm_handle* h, int b, const ClockArgs* ck = nullptr) {
   const Layout& L = h->lay;
   const long long face = std::max({(long long)L.ny * L.nz, (long long)L.nx * L.nz, (long long)L.nx * L.ny});
   // about one resident wave: blocks per face row up to 8 blocks/SM over all rows
@@ -483,8 +465,8 @@ cudaError_t launch_bc(fvm_handle* h, int b, const ClockArgs* ck = nullptr, int s
   const dim3 grid((unsigned)per_row, (unsigned)(6 * h->nv));
   const BcSpec bc = make_bc(h->d, h->nv);
   const ClockArgs c = ck ? *ck : ClockArgs{nullptr, 0, 0.0, 0.0, nullptr};
-  if (h->f64) bc_fill_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<double*>(h->U[b]), L, h->nv, bc, c, skip_x1);
-  else bc_fill_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<float*>(h->U[b]), L, h->nv, bc, c, skip_x1);
+  if (h->f64) bc_fill_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<double*>(h->U[b]), L, h->nv, bc, c);
+  else bc_fill_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<float*>(h->U[b]), L, h->nv, bc, c);
   return cudaGetLastError();
 }
 
@@ -551,7 +533,7 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
   const ClockArgs ck{h->clk, cmode, h->max_inv_l2, h->const_rate, h->status};
   const std::vector<StageDef> stages = stage_table(h->d.integrator);
   {
-    cudaError_t e = launch_bc(h, stages.front().in, &ck, x1_ring_sides(h));
+    cudaError_t e = launch_bc(h, stages.front().in, &ck);
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
   }
   if (h->closure) {
@@ -562,7 +544,7 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
   }
   bool first = true;
   for (const StageDef& sd : stages) {
-    cudaError_t e = first ? cudaSuccess : launch_bc(h, sd.in, nullptr, x1_ring_sides(h));
+    cudaError_t e = first ? cudaSuccess : launch_bc(h, sd.in);
     first = false;
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
     if ((rc = close(false))) return rc;

@@ -29,12 +29,6 @@ struct HeatParams {
   unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
   unsigned long long drain_ns;  // limit of the wait for copies in flight after a timeout (ns)
   unsigned extra_tx;  // test of the timeout path: bytes a ring copy never delivers (0 normally)
-  // x1 ghost faces formed in the TMA ring by the piecewise-constant kernel
-  // (bit s: side s, non-periodic) instead of by the ghost fill; kind and 2w
-  // of each side
-  int x1patch;
-  int x1kind[2];
-  float x1w2[2];
 };
 
 template <typename Real, int LIM, int TY>

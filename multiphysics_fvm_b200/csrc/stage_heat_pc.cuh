@@ -129,28 +129,6 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
           }
           got = g;
         }
-        // x1 ghost column of each newly landed interior plane from the
-        // adjacent interior column (non-periodic sides): the values the ghost
-        // fill would store, on the rows it fills (interior x2)
-        if (p.x1patch && got) {
-          for (int pl = (K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
-            if (pl < 1 || pl > nz) continue;
-            float* u = uring + pmod(pl, C::NSLOT) * C::SLOT;
-            for (int side = 0; side < 2; ++side) {
-              const int cg = side ? nx + 4 - x0 : 3 - x0;  // ring column of ghost x1 index 0 / nx+1
-              if (!((p.x1patch >> side) & 1) || cg < 0 || cg >= W) continue;
-              const int cs = side ? cg - 1 : cg + 1;      // the adjacent interior column
-              const int kind = p.x1kind[side];
-              const float w2 = p.x1w2[side];
-              for (int row = tid; row < C::ROWS; row += C::NT) {
-                const int gy = y0 + 1 - HH + row;
-                if (gy < 1 || gy > ny) continue;
-                const float v = u[row * W + cs];
-                u[row * W + cg] = kind == 2 ? -v : (kind == 3 ? w2 - v : v);
-              }
-            }
-          }
-        }
         if (!__syncthreads_and(got)) {
           if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
           return false;
