@@ -208,6 +208,9 @@ int fvm_batch_size(const fvm_batch* b, int* n, long long* tiles);
 int fvm_batch_handle(fvm_batch* b, int i, fvm_handle** h);
 int fvm_batch_step(fvm_batch* b, int n_steps, int dt_mode);
 int fvm_batch_time_steps(fvm_batch* b, int n_steps, int dt_mode, double* ms);
+/* Times the batch over z-march depths (and, for a mixed launch with heat grids,
+ * the heat tiles' heights, 20 or 10 rows) on the live states, restores them and
+ * keeps the fastest; fvm_tiling on a member handle reports its tile rows. */
 int fvm_batch_autotune(fvm_batch* b, int* best_zchunk, double* best_ms_per_step);
 /* Kernel launches per Runge-Kutta stage of one batched step.  It is 1 when every
  * grid is float32 and either inviscid cartesian navier_stokes (one limiter and

@@ -317,15 +317,19 @@ class Batch:
     ``setups`` are setup dicts (same integrator and precision; navier_stokes and
     heat may be mixed).  ``batch[i]`` is the i-th grid as a Simulation view."""
 
-    def __init__(self, setups):
+    def __init__(self, setups, heat_tile_rows: int = 0):
+        """``heat_tile_rows``: 10 puts the heat grids of a one-launch (mixed)
+        batch on 10-row tiles instead of 20 (``autotune`` times both)."""
         lib = L.load()
         descs = (L.FvmDesc * len(setups))()
         self.sims = []
         for i, s in enumerate(setups):
             sim = Simulation.__new__(Simulation)
-            descs[i] = sim._describe(physics_name(s["physics"]), s["coordinate_system"], s["grid_config"],
+            name = physics_name(s["physics"])
+            descs[i] = sim._describe(name, s["coordinate_system"], s["grid_config"],
                                      s["physical_parameters"], s["space_schemes"], s["boundary_conditions"],
-                                     s.get("time_integrator"), s.get("precision", "fp64"), 0, 0)
+                                     s.get("time_integrator"), s.get("precision", "fp64"), 0,
+                                     heat_tile_rows if name == "heat" else 0)
             self.sims.append(sim)
         b = C.c_void_p()
         L.check(lib.fvm_batch_create(descs, len(setups), C.byref(b)), "fvm_batch_create")

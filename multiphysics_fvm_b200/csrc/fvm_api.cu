@@ -1162,6 +1162,7 @@ struct fvm_batch {
     int physics = 0, lim = 0, riem = 0, coords = 0;
     bool visc = false;
     bool mixed = false;  // navier_stokes (lim, riem) and heat (coords) grids in one launch
+    int heat_ty = MIX_HEAT_TY;        // mixed: the heat members' tile rows
     std::vector<int> nbuf;            // mixed: staged tiles of each stage
     std::vector<int> members;
     std::vector<void*> prm;           // device params array per stage
@@ -1212,7 +1213,7 @@ int build_mixed_arrays(fvm_batch* b, fvm_batch::Group& g) {
         m.kind = 1;
         m.heat = make_heat_params<float>(h, st[si], false);
         m.heat.ntx = (h->lay.nx + 31) / 32;
-        m.heat.nty = (h->lay.ny + MIX_HEAT_TY - 1) / MIX_HEAT_TY;
+        m.heat.nty = (h->lay.ny + g.heat_ty - 1) / g.heat_ty;
         m.heat.nzc = (h->lay.nz + m.heat.zchunk - 1) / m.heat.zchunk;
         tiles = m.heat.ntx * m.heat.nty * m.heat.nzc;
       }
@@ -1286,7 +1287,7 @@ cudaError_t launch_group_stage(fvm_batch* b, fvm_batch::Group& g, int si, int ns
     const int nbuf = g.nbuf[si];
     const MixedSource src{static_cast<const MixedInst*>(g.prm[si]), g.tile_start, (int)g.members.size(),
                           mixed_bar_offset(nbuf)};
-    return launch_mixed(g.lim, g.riem, g.coords, src, g.ntiles, nbuf, b->stream, nsm);
+    return launch_mixed(g.lim, g.riem, g.coords, g.heat_ty, src, g.ntiles, nbuf, b->stream, nsm);
   }
   if (g.physics == FVM_NAVIER_STOKES) {
     BatchSource<NsParams<Real>> src{static_cast<const NsParams<Real>*>(g.prm[si]), g.maps[si], g.tile_start,
@@ -1416,6 +1417,9 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
   // float32 piecewise-constant heat (one coordinate system).
   bool mixed = true;
   int mlim = -1, mriem = -1, mcoords = -1;
+  // heat tile rows of a mixed launch: MIX_HEAT_TY, or MIX_HEAT_TY_ALT when the
+  // heat descriptors ask for it (tile_ty; the same in all of them)
+  int mheat_ty = 0;
   for (int i = 0; i < n && mixed; ++i) {
     const fvm_desc& d = descs[i];
     if (strip_desc(d) && d.params[1] == 0.0) {
@@ -1424,6 +1428,9 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     } else if (heat_pc_desc(d)) {
       if (mcoords < 0) mcoords = d.coords;
       mixed = d.coords == mcoords;
+      const int want = d.tile_ty == MIX_HEAT_TY_ALT ? MIX_HEAT_TY_ALT : MIX_HEAT_TY;
+      if (mheat_ty && want != mheat_ty) return bail(fail(FVM_E_INVALID, "batch: heat grids ask for different tile rows"));
+      mheat_ty = want;
     } else {
       mixed = false;
     }
@@ -1436,7 +1443,7 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     if (rc) return bail(rc);
     b->h.push_back(h);
     if (mixed) {  // the block shapes of the mixed launch's two bodies
-      h->tile_ty = heat_pc_desc(di) ? MIX_HEAT_TY : MIX_NS_TY;
+      h->tile_ty = heat_pc_desc(di) ? mheat_ty : MIX_NS_TY;
       if ((rc = make_tmaps(h))) return bail(rc);
     } else if (strip_desc(di) || heat_pc_desc(di)) {  // the tile-list kernels' shape, not the single-grid kernel's
       h->legacy = true;
@@ -1450,6 +1457,7 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     b->groups.emplace_back();
     fvm_batch::Group& g = b->groups.back();
     g.mixed = true;
+    g.heat_ty = mheat_ty ? mheat_ty : MIX_HEAT_TY;
     g.lim = std::max(mlim, 0);
     g.riem = std::max(mriem, 0);
     g.coords = std::max(mcoords, 0);
@@ -1681,8 +1689,27 @@ int fvm_batch_autotune(fvm_batch* b, int* best_zchunk, double* best_ms) {
   if (rc) return rc;
   int best = b->h[0]->zchunk;
   double bt = 1e30;
-  auto apply = [&](int z) -> int {
+  // heat tile rows of the mixed group (the other bodies have one shape)
+  fvm_batch::Group* mg = nullptr;
+  for (auto& g : b->groups)
+    if (g.mixed) mg = &g;
+  bool any_heat = false;
+  if (mg)
+    for (int i : mg->members) any_heat = any_heat || b->h[i]->d.physics == FVM_HEAT;
+  std::vector<int> heat_tys{mg ? mg->heat_ty : 0};
+  if (any_heat) heat_tys = {MIX_HEAT_TY, MIX_HEAT_TY_ALT};
+  int best_hty = heat_tys[0];
+  auto apply = [&](int z, int hty) -> int {
     for (fvm_handle* h : b->h) h->zchunk = z;
+    if (mg && mg->heat_ty != hty) {
+      mg->heat_ty = hty;
+      for (int i : mg->members) {
+        fvm_handle* h = b->h[i];
+        if (h->d.physics != FVM_HEAT) continue;
+        h->tile_ty = hty;
+        if (int r = make_tmaps(h)) return r;
+      }
+    }
     batch_drop_graphs(b);
     for (auto& g : b->groups) {
       const int r = b->f64 ? build_group_arrays<double>(b, g) : build_group_arrays<float>(b, g);
@@ -1690,16 +1717,19 @@ int fvm_batch_autotune(fvm_batch* b, int* best_zchunk, double* best_ms) {
     }
     return FVM_OK;
   };
-  for (int z : zchunk_candidates(nzmax)) {
-    if ((rc = apply(z))) break;
-    double ms = 0.0;
-    if ((rc = fvm_batch_time_steps(b, 1, 0, &ms))) break;
-    if ((rc = fvm_batch_time_steps(b, 3, 0, &ms))) break;
-    if (ms < bt) { bt = ms; best = z; }
-    if ((rc = restore_states(b->h, sv, false))) break;
+  for (int hty : heat_tys) {
+    for (int z : zchunk_candidates(nzmax)) {
+      if ((rc = apply(z, hty))) break;
+      double ms = 0.0;
+      if ((rc = fvm_batch_time_steps(b, 1, 0, &ms))) break;
+      if ((rc = fvm_batch_time_steps(b, 3, 0, &ms))) break;
+      if (ms < bt) { bt = ms; best = z; best_hty = hty; }
+      if ((rc = restore_states(b->h, sv, false))) break;
+    }
+    if (rc) break;
   }
   const int rr = restore_states(b->h, sv, true);
-  const int ra = apply(best);
+  const int ra = apply(best, best_hty);
   if (rc) return rc;
   if (rr) return rr;
   if (ra) return ra;

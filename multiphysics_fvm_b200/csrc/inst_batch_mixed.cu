@@ -1,10 +1,11 @@
-// Explicit instantiation: mixed navier_stokes + heat batch kernels (float32).
+// Explicit instantiation: mixed navier_stokes + heat batch kernels (float32),
+// 4-row heat strips (20-row heat tiles).
 #include "launch.cuh"
 namespace fvm {
-cudaError_t launch_mixed(int lim, int riem, int hcoord, const MixedSource& src, long long ntiles, int nbuf,
-                         cudaStream_t s, int nsm) {
+cudaError_t launch_mixed_h4(int lim, int riem, int hcoord, const MixedSource& src, long long ntiles, int nbuf,
+                            cudaStream_t s, int nsm) {
 #define FVM_MIX_CASE(L, R, CO) \
-  if (lim == L && riem == R && hcoord == CO) return launch_mixed_lrc<L, R, CO>(src, ntiles, nbuf, s, nsm);
+  if (lim == L && riem == R && hcoord == CO) return launch_mixed_lrc<L, R, CO, 4>(src, ntiles, nbuf, s, nsm);
 #define FVM_MIX_COORDS(L, R) FVM_MIX_CASE(L, R, COORD_CART) FVM_MIX_CASE(L, R, COORD_CYL) FVM_MIX_CASE(L, R, COORD_SPH)
   FVM_MIX_COORDS(LIM_PC, RIEM_RUSANOV)
   FVM_MIX_COORDS(LIM_PC, RIEM_HLL)

@@ -7,9 +7,10 @@ cudaError_t launch_heat_pc(int coord, const CUtensorMap& map, HeatParams<float> 
   p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
 #define FVM_HEAT_PC_CASE(CO)                                                                     \
   if (coord == CO)                                                                               \
-    return ty == HEAT_PC_TY_ALT ? launch_heat_pc_ty<CO, HEAT_PC_TY_ALT>(map, p, s, nsm)         \
-           : ty == MIX_HEAT_TY  ? launch_heat_pc_ty<CO, MIX_HEAT_TY>(map, p, s, nsm)            \
-                                : launch_heat_pc_ty<CO, HEAT_PC_TY>(map, p, s, nsm);
+    return ty == HEAT_PC_TY_ALT    ? launch_heat_pc_ty<CO, HEAT_PC_TY_ALT>(map, p, s, nsm)     \
+           : ty == MIX_HEAT_TY     ? launch_heat_pc_ty<CO, MIX_HEAT_TY>(map, p, s, nsm)        \
+           : ty == MIX_HEAT_TY_ALT ? launch_heat_pc_ty<CO, MIX_HEAT_TY_ALT>(map, p, s, nsm)    \
+                                   : launch_heat_pc_ty<CO, HEAT_PC_TY>(map, p, s, nsm);
   FVM_HEAT_PC_CASE(COORD_CART)
   FVM_HEAT_PC_CASE(COORD_CYL)
   FVM_HEAT_PC_CASE(COORD_SPH)

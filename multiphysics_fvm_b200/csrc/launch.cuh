@@ -272,12 +272,13 @@ cudaError_t launch_heat_any(int lim, int coord, const Src& src, long long ntiles
 }
 
 // Float32 piecewise-constant heat (stage_heat_pc.cuh): 4 rows per thread,
-// TY = 16 (4 warps) or 8 (2 warps).
+// TY = 16 (4 warps) or 8 (2 warps); mixed-batch members also run 20 (4 x 5
+// warps) and 10 (2-row strips, 5 warps).
 constexpr int HEAT_PC_TY = 16, HEAT_PC_TY_ALT = 8;
 
 template <int COORD, int TY>
 cudaError_t launch_heat_pc_ty(const CUtensorMap& map, const HeatParams<float>& p, cudaStream_t s, int nsm) {
-  constexpr int R = 4, NW = TY / R;
+  constexpr int R = TY % 4 == 0 ? 4 : 2, NW = TY / R;
   using C = HeatPcCfg<R, NW>;
   auto kern = heat_pc_kernel<COORD, R, NW>;
   static int bps = 0;
@@ -297,9 +298,9 @@ cudaError_t launch_heat_pc(int coord, const CUtensorMap& map, HeatParams<float> 
 
 // Mixed batch (stage_batch_mixed.cuh): navier_stokes (limiter, Riemann
 // solver) and heat (coordinate system) tiles in one launch.
-template <int LIM, int RIEM, int HCOORD>
+template <int LIM, int RIEM, int HCOORD, int HR>
 cudaError_t launch_mixed_lrc(const MixedSource& src, long long ntiles, int nbuf, cudaStream_t s, int nsm) {
-  auto kern = batch_mixed_kernel<LIM, RIEM, HCOORD>;
+  auto kern = batch_mixed_kernel<LIM, RIEM, HCOORD, HR>;
   static int bps[3] = {0, 0, 0};
   if (bps[0] == 0 || nsm < 0) {
     for (int nb = 0; nb < 3; ++nb) {
@@ -312,8 +313,16 @@ cudaError_t launch_mixed_lrc(const MixedSource& src, long long ntiles, int nbuf,
   kern<<<grid, MIX_NT, mixed_bytes(nbuf), s>>>(src);
   return cudaGetLastError();
 }
-cudaError_t launch_mixed(int lim, int riem, int hcoord, const MixedSource& src, long long ntiles, int nbuf,
-                         cudaStream_t s, int nsm);
+// heat_ty: the heat members' tile rows (MIX_HEAT_TY or MIX_HEAT_TY_ALT)
+cudaError_t launch_mixed_h4(int lim, int riem, int hcoord, const MixedSource& src, long long ntiles, int nbuf,
+                            cudaStream_t s, int nsm);
+cudaError_t launch_mixed_h2(int lim, int riem, int hcoord, const MixedSource& src, long long ntiles, int nbuf,
+                            cudaStream_t s, int nsm);
+inline cudaError_t launch_mixed(int lim, int riem, int hcoord, int heat_ty, const MixedSource& src, long long ntiles,
+                                int nbuf, cudaStream_t s, int nsm) {
+  return heat_ty == MIX_HEAT_TY_ALT ? launch_mixed_h2(lim, riem, hcoord, src, ntiles, nbuf, s, nsm)
+                                    : launch_mixed_h4(lim, riem, hcoord, src, ntiles, nbuf, s, nsm);
+}
 
 template <typename Real>
 cudaError_t launch_heat(int lim, int coord, const CUtensorMap& map, const HeatParams<Real>& p0, cudaStream_t s,

@@ -15,19 +15,19 @@
 
 namespace fvm {
 
-constexpr int MIX_NS_R = 2, MIX_NS_NW = 4;      // Navier-Stokes: 2-row strips, 8-row tiles
-constexpr int MIX_HEAT_R = 4, MIX_HEAT_NW = 5;  // heat: 4-row strips, 20-row tiles
+constexpr int MIX_NS_R = 2, MIX_NS_NW = 4;  // Navier-Stokes: 2-row strips, 8-row tiles
+constexpr int MIX_HEAT_NW = 5;              // heat: 4-row strips (20-row tiles) or 2-row (10-row tiles)
 constexpr int MIX_NT = 160;
 constexpr int MIX_NBAR = 7;
-constexpr int MIX_NS_TY = MIX_NS_R * MIX_NS_NW, MIX_HEAT_TY = MIX_HEAT_R * MIX_HEAT_NW;
-static_assert(NsStripCfg<MIX_NS_R, MIX_NS_NW>::NT == MIX_NT && HeatPcCfg<MIX_HEAT_R, MIX_HEAT_NW>::NT == MIX_NT,
+constexpr int MIX_NS_TY = MIX_NS_R * MIX_NS_NW, MIX_HEAT_TY = 4 * MIX_HEAT_NW, MIX_HEAT_TY_ALT = 2 * MIX_HEAT_NW;
+static_assert(NsStripCfg<MIX_NS_R, MIX_NS_NW>::NT == MIX_NT && HeatPcCfg<4, MIX_HEAT_NW>::NT == MIX_NT,
               "both bodies run on the same block");
 
 // Shared memory of a launch with `nbuf` staged Navier-Stokes tiles: the larger
 // body, then the barriers.
 __host__ __device__ constexpr int mixed_bar_offset(int nbuf) {
   return round_up(cmax(NsStripCfg<MIX_NS_R, MIX_NS_NW>::bytes(nbuf),
-                       HeatPcCfg<MIX_HEAT_R, MIX_HEAT_NW>::NSLOT * HeatPcCfg<MIX_HEAT_R, MIX_HEAT_NW>::SLOT * 4),
+                       HeatPcCfg<4, MIX_HEAT_NW>::NSLOT * HeatPcCfg<4, MIX_HEAT_NW>::SLOT * 4),
                   8);
 }
 __host__ __device__ constexpr int mixed_bytes(int nbuf) { return mixed_bar_offset(nbuf) + MIX_NBAR * 8; }
@@ -49,7 +49,8 @@ struct MixedSource {
   int bar_off;            // byte offset of the barriers in shared memory
 };
 
-template <int LIM, int RIEM, int HCOORD>
+// HR: heat rows per strip (4: 20-row heat tiles, 2: 10-row).
+template <int LIM, int RIEM, int HCOORD, int HR>
 __global__ void __launch_bounds__(MIX_NT, 3) batch_mixed_kernel(const __grid_constant__ MixedSource src) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + src.bar_off);
@@ -87,8 +88,7 @@ __global__ void __launch_bounds__(MIX_NT, 3) batch_mixed_kernel(const __grid_con
       }
     } else {
       if (in.heat.active && !*in.heat.active) continue;
-      if (!heat_pc_tile<HCOORD, MIX_HEAT_R, MIX_HEAT_NW>(in.heat, &in.tmap, tile, smem_raw, bars, phase_bits,
-                                                          pending)) {
+      if (!heat_pc_tile<HCOORD, HR, MIX_HEAT_NW>(in.heat, &in.tmap, tile, smem_raw, bars, phase_bits, pending)) {
         ok = false;
         break;
       }

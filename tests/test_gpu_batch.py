@@ -14,14 +14,18 @@ from tests.helpers import rel_l2
 pytestmark = pytest.mark.gpu
 
 
-def test_batch_matches_single_grids():
+@pytest.mark.parametrize("heat_rows", [0, 10])
+def test_batch_matches_single_grids(heat_rows):
+    """heat_rows 0: the heat grids on 20-row tiles (4-row strips), 10: 10-row
+    tiles (2-row strips)."""
     from multiphysics_fvm_b200.backend import Batch, Simulation
     from multiphysics_fvm_b200.setups import batch_mixed
     setups = batch_mixed.make_setups(seed=3, n_kh=5, n_heat=3, scale=0.15, n_steps=6)
     states = batch_mixed.initial_states(setups)
-    batch = Batch(setups)
+    batch = Batch(setups, heat_tile_rows=heat_rows)
     assert batch.tiles() > 0
     assert batch.launches_per_stage() == 1  # inviscid navier_stokes + heat: one mixed launch
+    assert batch[len(setups) - 1].tiling()[0] == (heat_rows or 20)
     for i, U in enumerate(states):
         batch[i].upload(U)
         batch[i].set_time(0.0, float("inf"), setups[i]["time_config"]["CFL"])
@@ -116,6 +120,9 @@ def test_autotune_restores_state():
     for i, U in enumerate(states):
         got = b[i].download()[:, 1:-1, 1:-1, 1:-1]
         assert np.array_equal(got, U.astype(np.float32).astype(np.float64)[:, 1:-1, 1:-1, 1:-1])
+    assert b[len(setups) - 1].tiling()[0] in (20, 10)  # the heat tiles' rows the sweep kept
+    b.step(2)
+    assert max(b[i].status() for i in range(len(setups))) == 0
     b.close()
 
 
