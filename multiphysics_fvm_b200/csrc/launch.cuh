@@ -195,16 +195,17 @@ cudaError_t launch_ns_strip_lr(NsStripSource& src, int ty, int nbuf, cudaStream_
 
 cudaError_t launch_ns_strip(int lim, int riem, NsStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm);
 
-// Viscous float32 cartesian grids (stage_ns_strip_visc.cuh): 2 rows per
-// thread, TY = 8 (4 output warps).  It is the second block shape of these
-// grids; the default one runs the general kernel (stage_ns.cuh).
+// Viscous float32 cartesian grids (stage_ns_strip_visc.cuh): 1 row per
+// thread, TY = 8 (8 output warps + the halo warp, 2 blocks/SM; 2-row strips
+// held 168 registers and ran 8 warps per SM).  It is the second block shape of
+// these grids; the default one runs the general kernel (stage_ns.cuh).
 constexpr int NS_STRIP_VISC_TY = 8;
 
 template <int LIM, int RIEM, int TY>
 cudaError_t launch_ns_strip_visc_ty(const NsStripSource& src, int nbuf, cudaStream_t s, int nsm) {
-  constexpr int R = 2, NW = TY / R;
+  constexpr int R = 1, NW = TY / R;
   using C = NsStripViscCfg<R, NW>;
-  auto kern = ns_strip_visc_kernel<LIM, RIEM, R, NW, TY == 8 ? 2 : 3>;
+  auto kern = ns_strip_visc_kernel<LIM, RIEM, R, NW, 2>;
   static int bps[3] = {0, 0, 0};
   if (bps[0] == 0 || nsm < 0) {
     for (int nb = 0; nb < 3; ++nb) {
