@@ -282,7 +282,8 @@ def run_ours(args):
     sim = Simulation.from_setup(s)
     sim.upload(U)
     sim.set_time(0.0, math.inf, 0.4)
-    zchunk, _ = sim.autotune()  # z-march depth for this grid (state restored)
+    zchunk, _ = sim.autotune()  # block shape and z-march depth for this grid (state restored)
+    tile_rows, _ = sim.tiling()
     cells = N_SIDE ** 3
 
     def barrier():
@@ -312,7 +313,12 @@ def run_ours(args):
     peak_source = "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650"
     # DRAM bytes per stage launch: not measured in this run; read from the
     # committed ncu capture (profiles/) and labelled with its source
-    traffic, traffic_source = profile_traffic("ns_stage_rt3d_256.md")
+    # the autotuner's two viscous shapes are two kernels: 7-row tiles run the
+    # register-blocked kernel, 6-row tiles the general one
+    strip = tile_rows == 7
+    kernel = ("ns_strip_visc_kernel (register-blocked residual + rk3 stage)" if strip
+              else "ns_stage_kernel (fused residual + rk3 stage)")
+    traffic, traffic_source = profile_traffic("ns_strip_visc_rt3d_256.md" if strip else "ns_stage_rt3d_256.md")
 
     # end to end through the public API with host buffers: every step uploads
     # the float64 ghosted state from pinned memory, advances one step and
@@ -349,14 +355,14 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "grid": [N_SIDE] * 3, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (each state buffer 345 MB > 126 MB)",
                        "timing": "CUDA events on the handle stream around K graph launches, max over ranks",
-                       "zchunk": zchunk},
+                       "tile_rows": tile_rows, "zchunk": zchunk},
             # per step: the CFL reduction, then per stage a ghost fill (the first one
             # also closes the clock) and the stage kernel
             "gpu_launches": args.steps * (1 + 2 * len(STAGE_BYTES)),
             "device_status": status,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_source,
-                         "kernel": "ns_stage_kernel (fused residual + rk3 stage)",
+                         "kernel": kernel,
                          "per_launch_ms": per_launch_ms, "alg_bytes_per_launch": alg_bytes,
                          "peak_source": peak_source},
             "step_breakdown_ms": {"stage_kernels": stage_ms / (launches / len(STAGE_BYTES)),

@@ -148,7 +148,7 @@ bool strip_desc(const fvm_desc& d) {
   return d.precision == FVM_FP32 && d.physics == FVM_NAVIER_STOKES && d.coords == FVM_CARTESIAN;
 }
 // viscous grids run it when the handle's block shape is the strip kernel's
-// (the autotuner's second shape); the default viscous shape is the general kernel's
+// (their default); the autotuner's second viscous shape is the general kernel's
 bool strip_kernel(const fvm_handle* h) {
   return !h->legacy && strip_desc(h->d) && (h->d.params[1] == 0.0 || h->tile_ty == NS_STRIP_VISC_TY);
 }
@@ -261,7 +261,7 @@ int kernel_limiter(const fvm_desc& d) {
 // one the float32 NS and heat kernels are also built with (equal if none).
 int default_tile_ty(const fvm_desc& d) {
   const bool f64 = d.precision == FVM_FP64, visc = d.physics == FVM_NAVIER_STOKES && d.params[1] != 0.0;
-  if (strip_desc(d)) return visc ? ns_tile_ty<float, true>() : NS_STRIP_TY;
+  if (strip_desc(d)) return visc ? NS_STRIP_VISC_TY : NS_STRIP_TY;
   if (heat_pc_desc(d)) return HEAT_PC_TY;
   if (d.physics == FVM_HEAT) return HEAT_TY;
   if (d.physics == FVM_MAXWELL) return f64 ? maxwell_tile_ty<double>() : MX_STRIP_TY;
@@ -273,7 +273,7 @@ int alt_tile_ty(const fvm_desc& d) {
   if (d.precision == FVM_FP64 || d.physics == FVM_MAXWELL) return default_tile_ty(d);
   if (heat_pc_desc(d)) return HEAT_PC_TY_ALT;
   if (d.physics == FVM_HEAT) return HEAT_TY_ALT;
-  if (strip_desc(d)) return d.params[1] != 0.0 ? NS_STRIP_VISC_TY : NS_STRIP_TY_ALT;
+  if (strip_desc(d)) return d.params[1] != 0.0 ? ns_tile_ty<float, true>() : NS_STRIP_TY_ALT;
   return d.params[1] != 0.0 ? ns_tile_ty_alt<float, true>() : ns_tile_ty_alt<float, false>();
 }
 // Halo rows staged on each side of a tile (TMA box height = rows + 2*halo).

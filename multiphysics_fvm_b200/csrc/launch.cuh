@@ -196,10 +196,12 @@ cudaError_t launch_ns_strip_lr(NsStripSource& src, int ty, int nbuf, cudaStream_
 cudaError_t launch_ns_strip(int lim, int riem, NsStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm);
 
 // Viscous float32 cartesian grids (stage_ns_strip_visc.cuh): 1 row per
-// thread, TY = 8 (8 output warps + the halo warp, 2 blocks/SM; 2-row strips
-// held 168 registers and ran 8 warps per SM).  It is the second block shape of
-// these grids; the default one runs the general kernel (stage_ns.cuh).
-constexpr int NS_STRIP_VISC_TY = 8;
+// thread, TY = 7 (7 output warps + the halo warp, 2 blocks/SM: 16 warps per SM,
+// 4 per scheduler, fit 128 registers without spills; 8 output warps left 96
+// registers and spilled, 2-row strips held 168 and ran 8 warps per SM).  It is
+// these grids' default block shape; the second one runs the general kernel
+// (stage_ns.cuh).
+constexpr int NS_STRIP_VISC_TY = 7;
 
 template <int LIM, int RIEM, int TY>
 cudaError_t launch_ns_strip_visc_ty(const NsStripSource& src, int nbuf, cudaStream_t s, int nsm) {

@@ -24,9 +24,9 @@ N = (70, 40, 13)
 CFG = dict(x1_min=0.0, x1_max=1.0, x2_min=0.0, x2_max=0.7, x3_min=0.0, x3_max=0.4, nx1=N[0], nx2=N[1], nx3=N[2])
 PRM = {"heat_capacity_ratio": 1.4, "dynamic_viscosity": 0.0, "gravitational_acceleration": [0.2, -0.1, 0.3]}
 # block shapes (tile rows) of each kernel: inviscid 8 (default) and 16; the
-# viscous strip kernel is the viscous grids' 8-row shape (their default 6-row
-# shape runs the general kernel)
-SHAPES = {0.0: (0, 16), 0.02: (8, 8)}
+# viscous strip kernel has one shape, the viscous grids' default 7 rows (their
+# 6-row shape runs the general kernel)
+SHAPES = {0.0: (0, 16), 0.02: (0, 7)}
 LIMITERS = [("piecewise_constant", None), ("muscl", "minmod"), ("muscl", "monotonized_central"),
             ("muscl", "van_leer")]
 WALLS = [["periodic"] * 2 + ["neumann", ("dirichlet", 1.7), "neumann", "neumann"],

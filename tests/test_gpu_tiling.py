@@ -47,7 +47,7 @@ def _state(c, rng):
     return to_fp32(random_ns_state(sh, rng))
 
 
-ALT_ROWS = [8, 16, 8]
+ALT_ROWS = [6, 16, 8]
 SAME_KERNEL = [False, True, True]  # viscous: the two shapes are two kernels
 
 
