@@ -1496,8 +1496,10 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     a.cmode = h->d.physics == FVM_NAVIER_STOKES ? 0 : 2;
     a.max_inv_l2 = h->max_inv_l2;
     a.const_rate = h->const_rate;
+    a.no_x3 = flat_grid(h) ? 1 : 0;
+    a.wide = bc_face_count(h->lay, h->nv, a.no_x3 != 0) >= (1ll << 31) ? 1 : 0;
     a.face_start = faces;
-    faces += bc_face_count(h->lay, h->nv);
+    faces += bc_face_count(h->lay, h->nv, a.no_x3 != 0);
   }
   b->faces = faces;
   if (cudaMalloc(&b->aux, n * sizeof(BatchAux)) != cudaSuccess ||

@@ -11,18 +11,21 @@ struct BcSpec {
 
 // Ghost face slabs of every variable (boundary_conditions.py:13-91 applied
 // per variable and side as in solver.py:30-37).  Edges and corners are never
-// read by the residual, so only the six face slabs are filled here.
-__host__ __device__ inline long long bc_face_count(const Layout& L, int nv) {
-  return 2ll * nv * ((long long)L.ny * L.nz + (long long)L.nx * L.nz + (long long)L.nx * L.ny);
+// read by the residual, so only the six face slabs are filled here; `no_x3`
+// leaves out the two x3 slabs (a one-plane grid whose stage kernel never reads
+// them).
+__host__ __device__ inline long long bc_face_count(const Layout& L, int nv, bool no_x3 = false) {
+  return 2ll * nv * ((long long)L.ny * L.nz + (long long)L.nx * L.nz + (no_x3 ? 0ll : (long long)L.nx * L.ny));
 }
 
 // Fill ghost element t (0 <= t < bc_face_count) of one grid.
 // Idx: the integer type of the element decomposition (32-bit whenever the
 // ghost count fits, which avoids emulated 64-bit division).
 template <typename Real, typename Idx = long long>
-__device__ __forceinline__ void bc_fill_one(Real* __restrict__ u, const Layout& L, const BcSpec& bc, Idx t) {
+__device__ __forceinline__ void bc_fill_one(Real* __restrict__ u, const Layout& L, const BcSpec& bc, Idx t,
+                                            bool no_x3 = false) {
   const Idx nyz = (Idx)L.ny * L.nz, nxz = (Idx)L.nx * L.nz, nxy = (Idx)L.nx * L.ny;
-  const Idx per_var = 2 * (nyz + nxz + nxy);
+  const Idx per_var = 2 * (nyz + nxz + (no_x3 ? 0 : nxy));
   {
     const int q = (int)(t / per_var);
     Idx r = t % per_var;
@@ -128,6 +131,8 @@ struct BatchAux {
   unsigned* status;
   BcSpec bc;
   int nv, cmode;  // clock mode (0 NS rates, 1 fixed, 2 constant)
+  int no_x3;      // one-plane grid whose kernels never read the x3 ghost slabs
+  int wide;       // the grid's ghost count does not fit 32 bits
   double max_inv_l2, const_rate;
   long long face_start;  // prefix sum of ghost elements
 };
@@ -143,7 +148,9 @@ __global__ void batch_bc_kernel(const BatchAux* __restrict__ a, int n, long long
     }
     const BatchAux& x = a[lo];
     if (!x.clk->active) continue;
-    bc_fill_one(static_cast<Real*>(x.U[buf]), x.lay, x.bc, t - x.face_start);
+    // the decode divides in 32 bits when the grid's ghost count fits
+    if (x.wide) bc_fill_one<Real, long long>(static_cast<Real*>(x.U[buf]), x.lay, x.bc, t - x.face_start, x.no_x3 != 0);
+    else bc_fill_one<Real, int>(static_cast<Real*>(x.U[buf]), x.lay, x.bc, (int)(t - x.face_start), x.no_x3 != 0);
   }
 }
 
