@@ -456,7 +456,9 @@ cudaError_t launch_stage(fvm_handle* h, const StageDef& sd, bool rhs_only, bool 
 }
 
 // Ghost fill of state buffer b; `ck` (optional) also closes the step's clock.
-cudaError_t launch_bc(fvm_handle* h, int b, const ClockArgs* ck = nullptr) {
+// `in_step`: a fill inside a step, which leaves out the x3 slabs of a
+// one-plane grid (its stage kernels never read them; downloads fill them).
+cudaError_t launch_bc(fvm_handle* h, int b, const ClockArgs* ck = nullptr, bool in_step = false) {
   const Layout& L = h->lay;
   const long long face = std::max({(long long)L.ny * L.nz, (long long)L.nx * L.nz, (long long)L.nx * L.ny});
   // about one resident wave: blocks per face row up to 8 blocks/SM over all rows
@@ -465,8 +467,9 @@ cudaError_t launch_bc(fvm_handle* h, int b, const ClockArgs* ck = nullptr) {
   const dim3 grid((unsigned)per_row, (unsigned)(6 * h->nv));
   const BcSpec bc = make_bc(h->d, h->nv);
   const ClockArgs c = ck ? *ck : ClockArgs{nullptr, 0, 0.0, 0.0, nullptr};
-  if (h->f64) bc_fill_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<double*>(h->U[b]), L, h->nv, bc, c);
-  else bc_fill_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<float*>(h->U[b]), L, h->nv, bc, c);
+  const int skip = in_step && flat_grid(h) ? (1 << 4) | (1 << 5) : 0;
+  if (h->f64) bc_fill_kernel<double><<<grid, 256, 0, h->stream>>>(static_cast<double*>(h->U[b]), L, h->nv, bc, c, skip);
+  else bc_fill_kernel<float><<<grid, 256, 0, h->stream>>>(static_cast<float*>(h->U[b]), L, h->nv, bc, c, skip);
   return cudaGetLastError();
 }
 
@@ -533,7 +536,7 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
   const ClockArgs ck{h->clk, cmode, h->max_inv_l2, h->const_rate, h->status};
   const std::vector<StageDef> stages = stage_table(h->d.integrator);
   {
-    cudaError_t e = launch_bc(h, stages.front().in, &ck);
+    cudaError_t e = launch_bc(h, stages.front().in, &ck, true);
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
   }
   if (h->closure) {
@@ -544,7 +547,7 @@ int enqueue_step(fvm_handle* h, int dt_mode, Prof* pf) {
   }
   bool first = true;
   for (const StageDef& sd : stages) {
-    cudaError_t e = first ? cudaSuccess : launch_bc(h, sd.in);
+    cudaError_t e = first ? cudaSuccess : launch_bc(h, sd.in, nullptr, true);
     first = false;
     if (e != cudaSuccess) return fail(FVM_E_CUDA, std::string("ghost fill: ") + cudaGetErrorString(e));
     if ((rc = close(false))) return rc;

@@ -336,14 +336,16 @@ struct ClockArgs {
 // block (0, 0) (ck.clk set).  The fill does not read the clock: filling the
 // ghosts of a state whose step turns out to be a no-op changes nothing a
 // later read sees (the ghost faces are a function of the interior, and
-// downloads fill them again).
+// downloads fill them again).  `skip_sides` (bit s) leaves out side s: the
+// x3 slabs of a one-plane grid, whose stage kernels never read them.
 constexpr int BCF = 4;
 template <typename Real>
-__global__ void __launch_bounds__(256) bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc, ClockArgs ck) {
+__global__ void __launch_bounds__(256) bc_fill_kernel(Real* __restrict__ u, Layout L, int nv, BcSpec bc, ClockArgs ck,
+                                                      int skip_sides) {
   if (ck.clk && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
     clock_one(ck.clk, ck.mode, ck.max_inv_l2, ck.const_rate, ck.status);
   const int q = blockIdx.y / 6, side = blockIdx.y % 6;
-  if (q >= nv) return;
+  if (q >= nv || ((skip_sides >> side) & 1)) return;
   const int axis = side >> 1, high = side & 1;
   const int A = axis == 0 ? L.ny : L.nx;  // along a row
   const int B = axis == 2 ? L.ny : L.nz;  // rows
