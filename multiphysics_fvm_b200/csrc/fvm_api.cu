@@ -384,6 +384,7 @@ NsParams<Real> make_ns_params(fvm_handle* h, const StageDef& sd, bool rhs_only) 
   p.g2 = d.params[3];
   p.g3 = d.params[4];
   p.flat = (!rhs_only && flat_grid(h)) ? 1 : 0;
+  p.ysub = 1;
   return p;
 }
 
@@ -1208,9 +1209,7 @@ int build_mixed_arrays(fvm_batch* b, fvm_batch::Group& g) {
         m.u0map = h->smap;
         m.accmap = h->amap;
         m.ns = make_ns_params<float>(h, st[si], false);
-        m.ns.ntx = (h->lay.nx + 31) / 32;
-        m.ns.nty = (h->lay.ny + MIX_NS_TY - 1) / MIX_NS_TY;
-        m.ns.nzc = (h->lay.nz + m.ns.zchunk - 1) / m.ns.zchunk;
+        ns_strip_tiles(m.ns, MIX_NS_TY);
         tiles = m.ns.ntx * m.ns.nty * m.ns.nzc;
       } else {
         m.kind = 1;

@@ -183,12 +183,20 @@ cudaError_t launch_ns_strip_ty(const NsStripSource& src, int nbuf, cudaStream_t 
   return cudaGetLastError();
 }
 
+// Row tiles a flat tile marches over along x2 (stage_ns_strip.cuh).
+constexpr int NS_FLAT_YSUB = 4;
+// Tile counts of the register-blocked kernel for block rows ty.
+inline void ns_strip_tiles(NsParams<float>& p, int ty) {
+  p.ntx = (p.lay.nx + 31) / 32;
+  p.ysub = p.flat ? NS_FLAT_YSUB : 1;
+  p.nty = ((p.lay.ny + ty - 1) / ty + p.ysub - 1) / p.ysub;
+  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
+}
+
 template <int LIM, int RIEM>
 cudaError_t launch_ns_strip_lr(NsStripSource& src, int ty, int nbuf, cudaStream_t s, int nsm) {
   NsParams<float>& p = src.p;
-  p.ntx = (p.lay.nx + 31) / 32;
-  p.nty = (p.lay.ny + ty - 1) / ty;
-  p.nzc = (p.lay.nz + p.zchunk - 1) / p.zchunk;
+  ns_strip_tiles(p, ty);
   if (ty == NS_STRIP_TY_ALT) return launch_ns_strip_ty<LIM, RIEM, NS_STRIP_TY_ALT>(src, nbuf, s, nsm);
   return launch_ns_strip_ty<LIM, RIEM, NS_STRIP_TY>(src, nbuf, s, nsm);
 }

@@ -34,6 +34,7 @@ struct NsParams {
   unsigned* status;
   int zchunk, ntx, nty, nzc;
   int flat;  // nx3 == 1 with x3 ghosts equal to the plane: x3 fluxes cancel, no z-march
+  int ysub;  // register-blocked kernel, flat grids: row tiles a tile marches over along x2
   unsigned long long wait_ns;  // limit of each wait for a TMA plane (ns)
   unsigned long long drain_ns;  // limit of the wait for copies in flight after a timeout (ns)
   unsigned extra_tx;  // test of the timeout path: bytes a ring copy never delivers (0 normally)

@@ -162,26 +162,35 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
     const int tx_i = tile % p.ntx;
     const int ty_i = (tile / p.ntx) % p.nty;
     const int zc_i = tile / (p.ntx * p.nty);
-    const int x0 = tx_i * TX, y0 = ty_i * TY;
     const int Z0 = 1 + zc_i * p.zchunk;         // first ghosted output plane
     const int Zl = min(Z0 + p.zchunk - 1, nz);  // last ghosted output plane
-    // a one-plane grid whose x3 ghosts copy the plane ("flat") has x3 fluxes
-    // that cancel exactly: plane 1 alone, no x3 pipeline
+    // A one-plane grid whose x3 ghosts copy the plane ("flat") has x3 fluxes
+    // that cancel exactly: plane 1 alone, no x3 pipeline.  Its tile marches
+    // instead over p.ysub row tiles along x2 (the steps of the march), each
+    // step's plane copy issued one step ahead into the next ring slot.
     const bool flat = p.flat != 0;
+    const int ysub = flat ? p.ysub : 1;
+    const int x0 = tx_i * TX, ybase = ty_i * ysub * TY;
+    int y0 = ybase;  // the current step's first row
+    const int nsteps = flat ? min(ysub, (ny + TY - 1) / TY - ty_i * ysub) : 0;
     const int Kfirst = flat ? Z0 : Z0 - 2, Plast = flat ? Zl : Zl + HH;
     const int i = x0 + lane;
     const float idx = (is_out && i < nx) ? __ldg(p.met.inv_dx1 + i) : 0.f;
 
-    auto issue = [&](int pl) {
-      const int s = pmod(pl, C::NSLOT);
+    // plane pl of the rows from yrow - HH into ring slot s
+    auto issue_at = [&](int pl, int s, int yrow) {
       pending |= 1u << s;
       fence_proxy_async();
       mbar_arrive_expect_tx(&bars[s], C::TX_BYTES + p.extra_tx);
-      tma_load_4d(&uring[s * C::SLOT], tmap, &bars[s], x0 - 3 + L.padx, y0 + 1 - HH, pl, 0);
+      tma_load_4d(&uring[s * C::SLOT], tmap, &bars[s], x0 - 3 + L.padx, yrow + 1 - HH, pl, 0);
     };
-    // planes Kfirst .. Kfirst + 2 (the first step's; a flat grid's one plane)
-    if (tid == 0)
-      for (int pl = Kfirst; pl <= (flat ? Kfirst : Kfirst + 2); ++pl) issue(pl);
+    auto issue = [&](int pl) { issue_at(pl, pmod(pl, C::NSLOT), y0); };
+    // planes Kfirst .. Kfirst + 2 (the first step's; a flat grid's first row tile)
+    if (tid == 0) {
+      if (flat) issue_at(Kfirst, 0, ybase);
+      else
+        for (int pl = Kfirst; pl <= Kfirst + 2; ++pl) issue(pl);
+    }
 
     // Halo warp: x1 data of plane Kh (ring plane uH, P plane pH) outside the
     // warps: lanes 0..TY-1 the slopes of the cell left of the tile, lanes
@@ -260,8 +269,11 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
       for (int v = 0; v < 5; ++v) fzp[r][v] = 0.f;
     }
 
-    for (int K = Kfirst, sK = pmod(Kfirst, C::NSLOT), pK0 = pmod(Kfirst, 3); K <= Zl;
-         ++K, sK = (sK == C::NSLOT - 1 ? 0 : sK + 1), pK0 = (pK0 == 2 ? 0 : pK0 + 1)) {
+    const int nstep = flat ? nsteps : Zl - Kfirst + 1;
+    for (int st = 0; st < nstep; ++st) {
+      const int K = flat ? Kfirst : Kfirst + st;
+      if (flat) y0 = ybase + st * TY;
+      const int sK = flat ? st % C::NSLOT : pmod(K, C::NSLOT), pK0 = flat ? 0 : pmod(K, 3);
       const bool outstep = K >= Z0;
       const int sK1 = sK == C::NSLOT - 1 ? 0 : sK + 1, sK2 = sK1 == C::NSLOT - 1 ? 0 : sK1 + 1;
       const int pK1i = pK0 == 2 ? 0 : pK0 + 1, pK2i = pK1i == 2 ? 0 : pK1i + 1;
@@ -273,7 +285,12 @@ __device__ __forceinline__ bool ns_strip_tile(const NsParams<float>& p, const CU
       float* pK2 = pring + pK2i * PL2;
       // ------------------------------------------------------------ 1 ----
       if (tid == 0) {
-        if (K > Kfirst && K + 2 <= Plast) issue(K + 2);
+        if (flat) {
+          // the next row tile's plane, into the slot two steps back left
+          if (st + 1 < nstep) issue_at(Kfirst, (st + 1) % C::NSLOT, y0 + TY);
+        } else if (K > Kfirst && K + 2 <= Plast) {
+          issue(K + 2);
+        }
         if (outstep && stg_bytes) {
           pending |= 1u << gbit;
           fence_proxy_async();
