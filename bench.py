@@ -284,6 +284,7 @@ def run_ours(args):
     sim.set_time(0.0, math.inf, 0.4)
     zchunk, _ = sim.autotune()  # block shape and z-march depth for this grid (state restored)
     tile_rows, _ = sim.tiling()
+    step_launches = sim.step_launches()  # the CFL reduction, ghost fills and stage kernels of one step
     cells = N_SIDE ** 3
 
     def barrier():
@@ -356,9 +357,9 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (each state buffer 345 MB > 126 MB)",
                        "timing": "CUDA events on the handle stream around K graph launches, max over ranks",
                        "tile_rows": tile_rows, "zchunk": zchunk},
-            # per step: the CFL reduction, then per stage a ghost fill (the first one
-            # also closes the clock) and the stage kernel
-            "gpu_launches": args.steps * (1 + 2 * len(STAGE_BYTES)),
+            # per step (fvm_step_launches): the CFL reduction, then per stage a
+            # ghost fill (the first one also closes the clock) and the stage kernel
+            "gpu_launches": args.steps * step_launches,
             "device_status": status,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_source,

@@ -168,6 +168,12 @@ int fvm_clear_status(fvm_handle* h);
  * (its only observability is the print of src/solver.py:147). */
 int fvm_set_wait_limit(fvm_handle* h, unsigned long long data_wait_ns, int never_complete);
 
+/* Kernel launches of one fvm_step step (dt_mode as in fvm_step): the CFL
+ * reduction (navier_stokes, dt_mode 0), then per stage a ghost fill (the first
+ * one also closes the step's clock) and the stage kernel; the closure's
+ * kernels (fvm_closure_attach) are not counted. */
+int fvm_step_launches(fvm_handle* h, int dt_mode, int* launches);
+
 /* Per-launch device time of the stage kernels (ms, CUDA events on the handle's
  * stream) over n_steps un-captured steps; fills per-stage totals. */
 int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_kernel_ms,

@@ -68,6 +68,7 @@ SIGNATURES = [
     ("fvm_status", C.c_int, [_P, C.POINTER(C.c_uint)]),
     ("fvm_clear_status", C.c_int, [_P]),
     ("fvm_set_wait_limit", C.c_int, [_P, C.c_ulonglong, C.c_int]),
+    ("fvm_step_launches", C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     ("fvm_profile_steps", C.c_int, [_P, C.c_int, C.c_int, _DP, _DP, C.POINTER(C.c_int)]),
     ("fvm_last_error", C.c_int, [C.c_char_p, C.c_int]),
     ("fvm_totals_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p]),

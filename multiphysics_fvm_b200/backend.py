@@ -293,6 +293,12 @@ class Simulation:
         L.check(self._lib.fvm_set_wait_limit(self._h, C.c_ulonglong(int(ns)), 1 if never_complete else 0),
                 "fvm_set_wait_limit")
 
+    def step_launches(self, dt_mode: int = 0) -> int:
+        """Kernel launches of one step: CFL reduction, ghost fills, stage kernels."""
+        n = C.c_int()
+        L.check(self._lib.fvm_step_launches(self._h, int(dt_mode), C.byref(n)), "fvm_step_launches")
+        return n.value
+
     def autotune(self):
         """Choose the z-march depth by timing candidates (state restored); returns (zchunk, ms/step)."""
         z, ms = C.c_int(), C.c_double()

@@ -1054,6 +1054,14 @@ int fvm_set_wait_limit(fvm_handle* h, unsigned long long data_wait_ns, int never
   return FVM_OK;
 }
 
+int fvm_step_launches(fvm_handle* h, int dt_mode, int* launches) {
+  if (!h || !launches) return fail(FVM_E_INVALID, "null handle or output");
+  // the launch sequence of enqueue_step, without the closure's kernels
+  const int stages = (int)stage_table(h->d.integrator).size();
+  *launches = (dt_mode == 0 && h->d.physics == FVM_NAVIER_STOKES ? 1 : 0) + 2 * stages;
+  return FVM_OK;
+}
+
 int fvm_profile_steps(fvm_handle* h, int n_steps, int dt_mode, double* stage_kernel_ms, double* other_kernel_ms,
                       int* stage_launches) {
   if (!h) return fail(FVM_E_INVALID, "null handle");

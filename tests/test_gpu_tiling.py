@@ -96,3 +96,19 @@ def test_unsupported_tile_rows_are_rejected():
     c = dict(c, coords="cartesian", grid=CFG)
     with pytest.raises(ValueError, match="tile_ty"):
         _sim(c, prm, 5)
+
+
+@pytest.mark.parametrize("integrator,stages", [("euler_explicit", 1), ("rk3_ssp", 3), ("rk4", 4)])
+def test_step_launches_match_the_profiled_launches(integrator, stages):
+    """fvm_step_launches (the bench line's gpu_launches) against the stage
+    launches that fvm_profile_steps counts: per step a CFL reduction
+    (navier_stokes), then per stage a ghost fill and the stage kernel."""
+    for k, (c, prm) in enumerate(CASES[1:]):
+        c = dict(c, coords="cartesian", grid=CFG)
+        sim = _sim(c, prm, 0, integrator=integrator)
+        sim.upload(_state(c, np.random.default_rng(5)))
+        sim.set_time(0.0, math.inf, 0.3)
+        _, _, launches = sim.profile_steps(2)
+        assert launches == 2 * stages
+        assert sim.step_launches() == (1 if c["physics"] == "navier_stokes" else 0) + 2 * stages
+        sim.close()
