@@ -1184,7 +1184,8 @@ struct fvm_batch {
   };
   std::vector<Group> groups;
   BatchAux* aux = nullptr;
-  long long faces = 0;
+  BcChunk* bc_chunks = nullptr;  // the ghost faces of all grids, BC_CHUNK cells per block
+  int n_chunks = 0;
   struct DtGroup {
     int coords = 0;
     BatchDt* d = nullptr;
@@ -1331,10 +1332,9 @@ int enqueue_batch_step(fvm_batch* b, int dt_mode) {
   batch_clock_kernel<<<(n + 127) / 128, 128, 0, b->stream>>>(b->aux, n, dt_mode == 1 ? 1 : 0);
   FVM_CK(cudaGetLastError());
   const std::vector<StageDef> st = stage_table(b->integrator);
-  const int bcb = (int)std::min<long long>((b->faces + 255) / 256, 8192);
   for (size_t si = 0; si < st.size(); ++si) {
-    if (b->f64) batch_bc_kernel<double><<<bcb, 256, 0, b->stream>>>(b->aux, n, b->faces, st[si].in);
-    else batch_bc_kernel<float><<<bcb, 256, 0, b->stream>>>(b->aux, n, b->faces, st[si].in);
+    if (b->f64) batch_bc_chunk_kernel<double><<<b->n_chunks, 256, 0, b->stream>>>(b->aux, b->bc_chunks, st[si].in);
+    else batch_bc_chunk_kernel<float><<<b->n_chunks, 256, 0, b->stream>>>(b->aux, b->bc_chunks, st[si].in);
     FVM_CK(cudaGetLastError());
     for (auto& g : b->groups) {
       cudaError_t e = b->f64 ? launch_group_stage<double>(b, g, (int)si, b->nsm)
@@ -1396,6 +1396,7 @@ int fvm_batch_destroy(fvm_batch* b) {
   for (auto& dg : b->dtg)
     if (dg.d) cudaFree(dg.d);
   if (b->aux) cudaFree(b->aux);
+  if (b->bc_chunks) cudaFree(b->bc_chunks);
   for (fvm_handle* h : b->h) fvm_destroy(h);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -1493,7 +1494,7 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
   }
   // auxiliary per-instance table and NS dt groups
   std::vector<BatchAux> aux(n);
-  long long faces = 0;
+  std::vector<BcChunk> chunks;
   for (int i = 0; i < n; ++i) {
     fvm_handle* h = b->h[i];
     BatchAux& a = aux[i];
@@ -1507,13 +1508,24 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     a.max_inv_l2 = h->max_inv_l2;
     a.const_rate = h->const_rate;
     a.no_x3 = flat_grid(h) ? 1 : 0;
-    a.wide = bc_face_count(h->lay, h->nv, a.no_x3 != 0) >= (1ll << 31) ? 1 : 0;
-    a.face_start = faces;
-    faces += bc_face_count(h->lay, h->nv, a.no_x3 != 0);
+    // the six face slabs of every variable (the two x3 slabs of a one-plane
+    // grid are never read by its stage kernels), in chunks of BC_CHUNK cells
+    const Layout& L = h->lay;
+    for (int q = 0; q < h->nv; ++q)
+      for (int side = 0; side < (a.no_x3 ? 4 : 6); ++side) {
+        const int axis = side >> 1;
+        const long long cells = axis == 0 ? (long long)L.ny * L.nz
+                                          : (axis == 1 ? (long long)L.nx * L.nz : (long long)L.nx * L.ny);
+        if (cells >= (1ll << 31)) return bail(fail(FVM_E_INVALID, "batch member: a ghost face exceeds 2^31 cells"));
+        for (long long s0 = 0; s0 < cells; s0 += BC_CHUNK)
+          chunks.push_back(BcChunk{i, q, side, (int)s0, (int)std::min<long long>(BC_CHUNK, cells - s0)});
+      }
   }
-  b->faces = faces;
+  b->n_chunks = (int)chunks.size();
   if (cudaMalloc(&b->aux, n * sizeof(BatchAux)) != cudaSuccess ||
-      cudaMemcpy(b->aux, aux.data(), n * sizeof(BatchAux), cudaMemcpyHostToDevice) != cudaSuccess)
+      cudaMemcpy(b->aux, aux.data(), n * sizeof(BatchAux), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMalloc(&b->bc_chunks, chunks.size() * sizeof(BcChunk)) != cudaSuccess ||
+      cudaMemcpy(b->bc_chunks, chunks.data(), chunks.size() * sizeof(BcChunk), cudaMemcpyHostToDevice) != cudaSuccess)
     return bail(fail(FVM_E_CUDA, "batch table upload failed"));
   for (int c = 0; c < 3; ++c) {
     std::vector<BatchDt> v;

@@ -9,49 +9,6 @@ struct BcSpec {
   double value[6][6];
 };
 
-// Ghost face slabs of every variable (boundary_conditions.py:13-91 applied
-// per variable and side as in solver.py:30-37).  Edges and corners are never
-// read by the residual, so only the six face slabs are filled here; `no_x3`
-// leaves out the two x3 slabs (a one-plane grid whose stage kernel never reads
-// them).
-__host__ __device__ inline long long bc_face_count(const Layout& L, int nv, bool no_x3 = false) {
-  return 2ll * nv * ((long long)L.ny * L.nz + (long long)L.nx * L.nz + (no_x3 ? 0ll : (long long)L.nx * L.ny));
-}
-
-// Fill ghost element t (0 <= t < bc_face_count) of one grid.
-// Idx: the integer type of the element decomposition (32-bit whenever the
-// ghost count fits, which avoids emulated 64-bit division).
-template <typename Real, typename Idx = long long>
-__device__ __forceinline__ void bc_fill_one(Real* __restrict__ u, const Layout& L, const BcSpec& bc, Idx t,
-                                            bool no_x3 = false) {
-  const Idx nyz = (Idx)L.ny * L.nz, nxz = (Idx)L.nx * L.nz, nxy = (Idx)L.nx * L.ny;
-  const Idx per_var = 2 * (nyz + nxz + (no_x3 ? 0 : nxy));
-  {
-    const int q = (int)(t / per_var);
-    Idx r = t % per_var;
-    int side, a, b;  // a, b: transverse interior indices (0-based)
-    if (r < 2 * nyz) { side = r < nyz ? 0 : 1; r %= nyz; a = (int)(r % L.ny); b = (int)(r / L.ny); }
-    else if ((r -= 2 * nyz) < 2 * nxz) { side = r < nxz ? 2 : 3; r %= nxz; a = (int)(r % L.nx); b = (int)(r / L.nx); }
-    else { r -= 2 * nxz; side = r < nxy ? 4 : 5; r %= nxy; a = (int)(r % L.nx); b = (int)(r / L.nx); }
-    const int kind = bc.kind[q][side];
-    const int axis = side >> 1, high = side & 1;
-    const int n = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
-    const int g = high ? n + 1 : 0;                       // ghost index along axis
-    const int inner = high ? n : 1;                       // adjacent interior
-    const int src = kind == 0 ? (high ? 1 : n) : inner;  // periodic: opposite layer
-    long long gi, si;
-    if (axis == 0) { gi = L.idx(q, b + 1, a + 1, g); si = L.idx(q, b + 1, a + 1, src); }
-    else if (axis == 1) { gi = L.idx(q, b + 1, g, a + 1); si = L.idx(q, b + 1, src, a + 1); }
-    else { gi = L.idx(q, g, b + 1, a + 1); si = L.idx(q, src, b + 1, a + 1); }
-    const Real v = u[si];
-    Real out;
-    if (kind == 2) out = -v;
-    else if (kind == 3) out = Real(2) * Real(bc.value[q][side]) - v;
-    else out = v;
-    u[gi] = out;
-  }
-}
-
 // Reference layout (C order, last axis fastest) <-> device layout (x1 fastest).
 // src/dst reference arrays have dims (nv, m1, m2, m3) and map to ghosted device
 // indices g = m + off.  32x32 shared-memory tiles over (x1, x3) per (var, x2).
@@ -132,27 +89,8 @@ struct BatchAux {
   BcSpec bc;
   int nv, cmode;  // clock mode (0 NS rates, 1 fixed, 2 constant)
   int no_x3;      // one-plane grid whose kernels never read the x3 ghost slabs
-  int wide;       // the grid's ghost count does not fit 32 bits
   double max_inv_l2, const_rate;
-  long long face_start;  // prefix sum of ghost elements
 };
-
-template <typename Real>
-__global__ void batch_bc_kernel(const BatchAux* __restrict__ a, int n, long long total, int buf) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (a[mid].face_start <= t) lo = mid; else hi = mid - 1;
-    }
-    const BatchAux& x = a[lo];
-    if (!x.clk->active) continue;
-    // the decode divides in 32 bits when the grid's ghost count fits
-    if (x.wide) bc_fill_one<Real, long long>(static_cast<Real*>(x.U[buf]), x.lay, x.bc, t - x.face_start, x.no_x3 != 0);
-    else bc_fill_one<Real, int>(static_cast<Real*>(x.U[buf]), x.lay, x.bc, (int)(t - x.face_start), x.no_x3 != 0);
-  }
-}
 
 __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) {
   atomicMax(a, (unsigned long long)__double_as_longlong(v));
@@ -373,6 +311,50 @@ __global__ void __launch_bounds__(256) bc_fill_kernel(Real* __restrict__ u, Layo
     for (int m = 0; m < BCF; ++m)
       if (t0 + m * stride < total) u[gi[m]] = kind == 2 ? -v[m] : (kind == 3 ? two_w - v[m] : v[m]);
   }
+}
+
+// A batch's ghost faces as a static list of chunks: up to BC_CHUNK
+// consecutive cells of one face slab (grid, variable, side), one block each,
+// so a block needs no search for its grid and no per-cell decode of the slab.
+constexpr int BC_CHUNK = 256 * BCF;
+struct BcChunk {
+  int grid, q, side, start, count;
+};
+
+// The ghost faces (bc_fill_kernel's arithmetic) of the chunks' state buffer
+// `buf`; grids whose clock passed t_end are skipped.
+template <typename Real>
+__global__ void __launch_bounds__(256) batch_bc_chunk_kernel(const BatchAux* __restrict__ a,
+                                                             const BcChunk* __restrict__ ch, int buf) {
+  const BcChunk c = ch[blockIdx.x];
+  const BatchAux& x = a[c.grid];
+  if (!x.clk->active) return;
+  Real* __restrict__ u = static_cast<Real*>(x.U[buf]);
+  const Layout& L = x.lay;
+  const int q = c.q, side = c.side, axis = side >> 1, high = side & 1;
+  const int A = axis == 0 ? L.ny : L.nx;  // along a row
+  const int kind = x.bc.kind[q][side];
+  const int n = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
+  const int g = high ? n + 1 : 0;                       // ghost index along axis
+  const int inner = high ? n : 1;                       // adjacent interior
+  const int src = kind == 0 ? (high ? 1 : n) : inner;  // periodic: opposite layer
+  const Real two_w = Real(2) * Real(x.bc.value[q][side]);
+  Real v[BCF];
+  long long gi[BCF];
+#pragma unroll
+  for (int m = 0; m < BCF; ++m) {
+    const int k = threadIdx.x + m * 256;
+    const int t = c.start + k;
+    const int a0 = t % A, b0 = t / A;
+    long long si;
+    if (axis == 0) { gi[m] = L.idx(q, b0 + 1, a0 + 1, g); si = L.idx(q, b0 + 1, a0 + 1, src); }
+    else if (axis == 1) { gi[m] = L.idx(q, b0 + 1, g, a0 + 1); si = L.idx(q, b0 + 1, src, a0 + 1); }
+    else { gi[m] = L.idx(q, g, b0 + 1, a0 + 1); si = L.idx(q, src, b0 + 1, a0 + 1); }
+    v[m] = k < c.count ? u[si] : Real(0);
+  }
+#pragma unroll
+  for (int m = 0; m < BCF; ++m)
+    if (threadIdx.x + m * 256 < c.count) u[gi[m]] = kind == 2 ? -v[m] : (kind == 3 ? two_w - v[m] : v[m]);
 }
 
 __global__ void batch_clock_kernel(const BatchAux* __restrict__ a, int n, int fixed) {

@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(MIX_NT, 3) batch_mixed_kernel(const __grid_con
       }
     } else {
       if (in.heat.active && !*in.heat.active) continue;
-      if (!heat_pc_tile<HCOORD, HR, MIX_HEAT_NW>(in.heat, &in.tmap, tile, smem_raw, bars, phase_bits, pending)) {
+      if (!heat_pc_tile<HCOORD, HR, MIX_HEAT_NW, true>(in.heat, &in.tmap, tile, smem_raw, bars, phase_bits, pending)) {
         ok = false;
         break;
       }

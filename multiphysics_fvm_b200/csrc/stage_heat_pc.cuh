@@ -36,7 +36,11 @@ struct HeatPcCfg {
 // One tile of the stage (all planes of its z-chunk) with the ring barriers
 // `bars` (phase bits 0..5); `phase_bits` and `pending` carry over from tile to
 // tile.  Returns false when a wait ran out: the block must stop and drain.
-template <int COORD, int R, int NW>
+// MERGED: the two warm-up steps of the z-march (phi3 of planes Z0-1 and Z0)
+// are one prologue step.  It pays where z-chunks are short and many (the
+// batched launch); a single-grid launch of one wave of long chunks ran 2 %
+// slower with it.
+template <int COORD, int R, int NW, bool MERGED = false>
 __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const CUtensorMap* tmap, int tile,
                                              unsigned char* smem_raw, uint64_t* bars, unsigned& phase_bits,
                                              unsigned& pending) {
@@ -98,13 +102,53 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
       g3[r] = -0.5f * kap;
       if constexpr (COORD == COORD_SPH) g3[r] *= __ldg(m.inv_r + ic) * __ldg(m.inv_sin_c2 + jc);
     }
+    // phi3 of plane P at the own cells from the ring planes P-1 (um) and P+1
+    // (up); zero on a ghost plane
+    auto phi3 = [&](int P, const float* um, const float* up, float* out) {
+      const bool zg = P <= 0 || P >= nz + 1;
+      const float idz1 = zg ? 0.f : __ldg(m.inv_dx3 + min(max(P - 1, 0), nz - 1));
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int o = (w * R + r + HH) * W + lane + 4;
+        out[r] = (g3[r] * idz1) * (up[o] - um[o]);
+      }
+    };
     float phz0[R], phz1[R];  // phi3 of planes K-1 and K at the own cells
 #pragma unroll
     for (int r = 0; r < R; ++r) { phz0[r] = 0.f; phz1[r] = 0.f; }
+    if constexpr (MERGED) {
+      // prologue: planes Z0-2 .. Z0+1 give phi3 of planes Z0-1 and Z0 in one
+      // step (one wait round and one barrier pair for both)
+      bool got = true;
+      for (int pl = Kfirst; pl <= Kfirst + 3; ++pl) {
+        const int s = pmod(pl, C::NSLOT);
+        const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
+        if (g) {
+          phase_bits ^= 1u << s;
+          if (tid == 0) pending &= ~(1u << s);
+        }
+        got = g;
+      }
+      if (!__syncthreads_and(got)) {
+        if (tid == 0) atomicOr(p.status, ST_TMA_TIMEOUT);
+        return false;
+      }
+      phi3(Z0 - 1, uring + pmod(Kfirst, C::NSLOT) * C::SLOT, uring + pmod(Kfirst + 2, C::NSLOT) * C::SLOT, phz0);
+      phi3(Z0, uring + pmod(Kfirst + 1, C::NSLOT) * C::SLOT, uring + pmod(Kfirst + 3, C::NSLOT) * C::SLOT, phz1);
+      __syncthreads();  // planes Z0-2 and Z0-1 are refilled at the first step
+    }
 
-    for (int K = Kfirst, sK = pmod(Kfirst, C::NSLOT); K <= Zl; ++K, sK = (sK == C::NSLOT - 1 ? 0 : sK + 1)) {
-      if (tid == 0 && K > Kfirst && K + C::NSLOT - 1 <= Plast) issue(K + C::NSLOT - 1);
-      const bool outstep = K >= Z0;
+    const int K0 = MERGED ? Z0 : Kfirst;
+    int next_pl = Kfirst + C::NSLOT;  // MERGED: the next plane to issue (thread 0)
+    for (int K = K0, sK = pmod(K0, C::NSLOT); K <= Zl; ++K, sK = (sK == C::NSLOT - 1 ? 0 : sK + 1)) {
+      if constexpr (MERGED) {
+        // the prologue freed two slots: the first step refills both
+        if (tid == 0)
+          for (; next_pl <= K + C::NSLOT - 1 && next_pl <= Plast; ++next_pl) issue(next_pl);
+      } else {
+        if (tid == 0 && K > Kfirst && K + C::NSLOT - 1 <= Plast) issue(K + C::NSLOT - 1);
+      }
+      const bool outstep = MERGED || K >= Z0;  // the merged loop starts at Z0
       // U0 / acc of the plane's own cells, loaded before anything is stored
       // in this step so that the step hides their latency
       float eu0[R], eacc[R];
@@ -120,7 +164,7 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
       }
       {
         bool got = true;
-        for (int pl = (K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
+        for (int pl = (!MERGED && K == Kfirst ? Kfirst : K + 2); pl <= K + 2; ++pl) {
           const int s = pmod(pl, C::NSLOT);
           const bool g = got && mbar_wait_bounded(&bars[s], (phase_bits >> s) & 1u, p.wait_ns);
           if (g) {
@@ -137,15 +181,18 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
       const int s2 = sK + 2 >= C::NSLOT ? sK + 2 - C::NSLOT : sK + 2;
       const float* uK = uring + sK * C::SLOT;
       const float* uK2 = uring + s2 * C::SLOT;
-      // phi3 of plane K+1 at the own cells (zero on a ghost plane); 1/dx3 of
-      // interior plane K (ghosted K+1)
-      const bool zg = K + 1 <= 0 || K + 1 >= nz + 1;
-      const float idz1 = zg ? 0.f : __ldg(m.inv_dx3 + min(max(K, 0), nz - 1));
-      float phz2[R];
+      float phz2[R];  // phi3 of plane K+1 at the own cells (zero on a ghost plane)
+      if constexpr (MERGED) {
+        phi3(K + 1, uK, uK2, phz2);
+      } else {
+        // 1/dx3 of interior plane K (ghosted K+1)
+        const bool zg = K + 1 <= 0 || K + 1 >= nz + 1;
+        const float idz1 = zg ? 0.f : __ldg(m.inv_dx3 + min(max(K, 0), nz - 1));
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int o = (w * R + r + HH) * W + lane + 4;
-        phz2[r] = (g3[r] * idz1) * (uK2[o] - uK[o]);
+        for (int r = 0; r < R; ++r) {
+          const int o = (w * R + r + HH) * W + lane + 4;
+          phz2[r] = (g3[r] * idz1) * (uK2[o] - uK[o]);
+        }
       }
       if (outstep) {
         const float idz = __ldg(m.inv_dx3 + (K - 1));
