@@ -1190,6 +1190,8 @@ struct fvm_batch {
     int coords = 0;
     BatchDt* d = nullptr;
     int n = 0;
+    DtBlock* blk = nullptr;  // the reduction's blocks (DT_CELLS cells each)
+    int nblk = 0;
   };
   std::vector<DtGroup> dtg;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -1314,8 +1316,7 @@ int enqueue_batch_step(fvm_batch* b, int dt_mode) {
   const int n = (int)b->h.size();
   if (dt_mode == 0) {
     for (auto& dg : b->dtg) {
-      dim3 grid(32, dg.n);
-#define FVM_BDT(R, C) batch_ns_dt_kernel<R, C><<<grid, 256, 0, b->stream>>>(dg.d)
+#define FVM_BDT(R, C) batch_ns_dt_kernel<R, C><<<dg.nblk, 256, 0, b->stream>>>(dg.d, dg.blk)
       if (b->f64) {
         if (dg.coords == FVM_CARTESIAN) FVM_BDT(double, COORD_CART);
         else if (dg.coords == FVM_CYLINDRICAL) FVM_BDT(double, COORD_CYL);
@@ -1393,8 +1394,10 @@ int fvm_batch_destroy(fvm_batch* b) {
     for (CUtensorMap* x : g.maps) cudaFree(x);
     if (g.tile_start) cudaFree(g.tile_start);
   }
-  for (auto& dg : b->dtg)
+  for (auto& dg : b->dtg) {
     if (dg.d) cudaFree(dg.d);
+    if (dg.blk) cudaFree(dg.blk);
+  }
   if (b->aux) cudaFree(b->aux);
   if (b->bc_chunks) cudaFree(b->bc_chunks);
   for (fvm_handle* h : b->h) fvm_destroy(h);
@@ -1529,19 +1532,28 @@ int fvm_batch_create(const fvm_desc* descs, int n, fvm_batch** out) {
     return bail(fail(FVM_E_CUDA, "batch table upload failed"));
   for (int c = 0; c < 3; ++c) {
     std::vector<BatchDt> v;
+    std::vector<DtBlock> blk;
     for (int i = 0; i < n; ++i) {
       fvm_handle* h = b->h[i];
       if (h->d.physics != FVM_NAVIER_STOKES || h->d.coords != c) continue;
+      const long long cells = (long long)h->lay.nx * h->lay.ny * h->lay.nz;
+      const int nbx = (int)std::max(1LL, std::min((cells + DT_CELLS - 1) / DT_CELLS, 3LL * b->nsm));
+      for (int k = 0; k < nbx; ++k) blk.push_back(DtBlock{(int)v.size(), k, nbx});
       v.push_back(BatchDt{h->U[0], h->lay, h->md, h->d.params[0], h->d.params[1], h->clk, h->status});
     }
     if (v.empty()) continue;
     fvm_batch::DtGroup dg;
     dg.coords = c;
     dg.n = (int)v.size();
-    if (cudaMalloc(&dg.d, v.size() * sizeof(BatchDt)) != cudaSuccess ||
-        cudaMemcpy(dg.d, v.data(), v.size() * sizeof(BatchDt), cudaMemcpyHostToDevice) != cudaSuccess)
-      return bail(fail(FVM_E_CUDA, "batch dt table upload failed"));
+    dg.nblk = (int)blk.size();
+    // owned by the batch from here on (freed by fvm_batch_destroy on every path)
     b->dtg.push_back(dg);
+    fvm_batch::DtGroup& g = b->dtg.back();
+    if (cudaMalloc(&g.d, v.size() * sizeof(BatchDt)) != cudaSuccess ||
+        cudaMemcpy(g.d, v.data(), v.size() * sizeof(BatchDt), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMalloc(&g.blk, blk.size() * sizeof(DtBlock)) != cudaSuccess ||
+        cudaMemcpy(g.blk, blk.data(), blk.size() * sizeof(DtBlock), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(FVM_E_CUDA, "batch dt table upload failed"));
   }
   *out = b;
   return FVM_OK;

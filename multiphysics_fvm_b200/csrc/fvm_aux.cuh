@@ -98,18 +98,28 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long* a, double v) 
 
 // CFL rates of the Navier-Stokes state (navier_stokes.py:512-585) in float64:
 // red[0] = max_cells max_d max_w |v_d + kappa_w| / L_d, red[1] = max mu/rho.
+// Block bx of the nbx blocks that share the grid.
 template <typename Real, int COORD>
 __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, const Layout& L, const Metric<double>& m,
-                                                  double gam, double mu, Clock* clk, unsigned* status);
+                                                  double gam, double mu, Clock* clk, unsigned* status, int bx,
+                                                  int nbx);
 
 template <typename Real, int COORD>
 __global__ void __launch_bounds__(256, 3)
     ns_dt_reduce_kernel(const Real* __restrict__ u, Layout L, Metric<double> m, double gam, double mu, Clock* clk,
                         unsigned* status) {
-  ns_dt_reduce_body<Real, COORD>(u, L, m, gam, mu, clk, status);
+  ns_dt_reduce_body<Real, COORD>(u, L, m, gam, mu, clk, status, blockIdx.x, gridDim.x);
 }
 
-// Per-instance CFL rates of a batch of Navier-Stokes grids: blockIdx.y picks the grid.
+// Per-instance CFL rates of a batch of Navier-Stokes grids: a static list of
+// blocks, each grid's count proportional to its cells (DT_CELLS per block, at
+// least one), so a large grid does not leave one block per SM working while
+// the small grids' blocks have finished.  The maximum does not depend on the
+// split: the dt is bitwise that of the single-grid reduction.
+constexpr int DT_CELLS = 2048;
+struct DtBlock {
+  int grid, bx, nbx;
+};
 struct BatchDt {
   const void* u;
   Layout lay;
@@ -119,14 +129,18 @@ struct BatchDt {
   unsigned* status;
 };
 template <typename Real, int COORD>
-__global__ void batch_ns_dt_kernel(const BatchDt* __restrict__ b) {
-  const BatchDt& x = b[blockIdx.y];
-  ns_dt_reduce_body<Real, COORD>(static_cast<const Real*>(x.u), x.lay, x.md, x.gam, x.mu, x.clk, x.status);
+__global__ void __launch_bounds__(256, 3) batch_ns_dt_kernel(const BatchDt* __restrict__ b,
+                                                             const DtBlock* __restrict__ blk) {
+  const DtBlock k = blk[blockIdx.x];
+  const BatchDt& x = b[k.grid];
+  ns_dt_reduce_body<Real, COORD>(static_cast<const Real*>(x.u), x.lay, x.md, x.gam, x.mu, x.clk, x.status, k.bx,
+                                 k.nbx);
 }
 
 template <typename Real, int COORD>
 __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, const Layout& L, const Metric<double>& m,
-                                                  double gam, double mu, Clock* clk, unsigned* status) {
+                                                  double gam, double mu, Clock* clk, unsigned* status, int bx,
+                                                  int nbx) {
   if (!clk->active) return;
   __shared__ double s_rc[32], s_nu[32];
   double rc = 0.0, nu = 0.0;
@@ -140,8 +154,8 @@ __device__ __forceinline__ void ns_dt_reduce_body(const Real* __restrict__ u, co
   constexpr int IB = 2;
   const int nch = (L.nx + 31) >> 5;
   const int lane = threadIdx.x & 31;
-  const int nwarp = gridDim.x * (blockDim.x >> 5);
-  const int w0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int nwarp = nbx * (blockDim.x >> 5);
+  const int w0 = bx * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int dq = nwarp / nch, dr = nwarp % nch, rj = dq % L.ny, rk = dq / L.ny;
   int cc = w0 % nch, cj = (w0 / nch) % L.ny, ck = (w0 / nch) / L.ny;  // load cursor
   auto advance = [&]() {
