@@ -155,3 +155,32 @@ def test_batch_members_against_oracle():
         e = rel_l2(b[i].download()[I3], Uo[I3])
         assert e <= 1e-5, (i, physics_name(s["physics"]), e)
     b.close()
+
+
+def test_batch_cfl_dt_bitwise_single_grid():
+    """The batch's CFL reduction splits each grid over blocks in proportion to
+    its cells; the maximum does not depend on the split, so the first step's dt
+    of every navier_stokes member equals the single grid's bitwise (the grids
+    span one to several reduction blocks)."""
+    from multiphysics_fvm_b200.backend import Batch, Simulation
+    from multiphysics_fvm_b200.setups import batch_mixed
+    setups = batch_mixed.make_setups(seed=5, n_kh=6, n_heat=2, scale=0.3, n_steps=1)
+    states = batch_mixed.initial_states(setups)
+    batch = Batch(setups)
+    for i, U in enumerate(states):
+        batch[i].upload(U)
+        batch[i].set_time(0.0, float("inf"), setups[i]["time_config"]["CFL"])
+    batch.step(1)
+    sizes = []
+    for i, (s, U) in enumerate(zip(setups, states)):
+        if s["grid_config"]["nx3"] != 1:
+            continue
+        sizes.append(s["grid_config"]["nx1"] * s["grid_config"]["nx2"])
+        sim = Simulation.from_setup(s)
+        sim.upload(U)
+        sim.set_time(0.0, float("inf"), s["time_config"]["CFL"])
+        sim.step(1)
+        assert batch[i].time()[2] == sim.time()[2], (i, batch[i].time(), sim.time())
+        sim.close()
+    batch.close()
+    assert max(sizes) > 2 * 2048 and min(sizes) < 2048, sizes
