@@ -118,7 +118,7 @@ __device__ __forceinline__ bool heat_pc_tile(const HeatParams<float>& p, const C
     for (int r = 0; r < R; ++r) { phz0[r] = 0.f; phz1[r] = 0.f; }
     if constexpr (MERGED) {
       // prologue: planes Z0-2 .. Z0+1 give phi3 of planes Z0-1 and Z0 in one
-      // step (one wait round and one barrier pair for both)
+      // step (one set of waits and one barrier pair for both)
       bool got = true;
       for (int pl = Kfirst; pl <= Kfirst + 3; ++pl) {
         const int s = pmod(pl, C::NSLOT);
